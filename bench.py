@@ -1,0 +1,303 @@
+"""Benchmark: cells/s of one GCM chemistry call on the 69-species network, 1,048,576 cells per GPU.
+
+Workload: the seeded synthetic 69-species C-H-N-O network (390 reactions, 48 photolysis branches) on a column grid of
+64 log-P levels (1e-2 to 1e8 dyn cm^-2) x 16,384 columns, T a smooth 400-2200 K profile with +-100 K noise, upper-layer
+J log-uniform in 1e-10..1e-3 s^-1 where P < 1e3. Four untimed 300 s calls from a solar-like start settle the gas; a
+step is then the fifth 300 s call (x, T, P, dt, h, J resident in HBM), repeated on the same inputs. The inputs
+(552 MB of x alone) exceed L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--cells B] [--impl ours|reference]
+
+--impl reference times the CPU implementation of the same solve (the oracle, a C restatement of the reference's
+kernels, on all host threads) on a bounded sample of the same cells; rank 0 alone runs it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cells/s per GCM call (69-sp, 1M cells): FP64 Rodas3 vs mixed/learned @rtol 1e-3"
+NETWORK = "chno69"
+LEVELS = 64
+SPINUP_CALLS = 4
+DT = 300.0
+
+
+def parse() -> argparse.Namespace:
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--cells", type=int, default=1 << 20, help="cells per GPU")
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--cpu-sample", type=int, default=2048, help="cells of the CPU baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def inputs(net, cells: int, seed: int):
+    from maxichem_b200 import synthetic
+
+    return synthetic.workload(net, "column", cells, seed=seed)
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int) -> None:
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)  # fmt: skip
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([q.strip() for q in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = [r for r in self.rows if len(r) == 7]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = [n for k, n in enumerate(names) if any(r[3 + k].lower() == "active" for r in rows)]
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][1]) if rows[0][1] else None,
+                "reasons": reasons, "samples": len(rows)}  # fmt: skip
+
+
+def run_reference(args) -> None:
+    """The CPU implementation of the same solve on the host's cores, one bounded sample per step."""
+    import oracle
+    from maxichem_b200 import synthetic, tables
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    net = synthetic.network(NETWORK)
+    tab = tables.build(net, True)
+    ref = oracle.Oracle(tab)
+    sample = min(args.cpu_sample, args.cells)
+    w = inputs(net, sample, seed=7)
+    x, h = w.x, w.h
+    for _ in range(SPINUP_CALLS):
+        r = ref.call(x, w.T, w.P, w.dt, h, J=w.J)
+        x, h = r["x"], r["h"]
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ref.call(x, w.T, w.P, w.dt, h, J=w.J)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = sample / float(np.mean(times))
+    cores = oracle.threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{NETWORK} column grid, call {SPINUP_CALLS + 1} of 300 s calls", "cells": sample,
+                   "species": tab.ns, "reactions": tab.nr},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "port",
+                         "sample": f"{sample} cells of the same call, all {cores} host threads (OpenMP)"},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from maxichem_b200 import abi, synthetic
+    from maxichem_b200.solver import CudaSolver, check_inputs
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    net = synthetic.network(NETWORK)
+    B = args.cells
+    w = inputs(net, B, seed=1000 + rank)  # each rank its own shard of columns
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    solver = CudaSolver(net, dev, photo=True)
+    tab = solver.tab
+    x, T, P, dt, h, J = t(w.x), t(w.T), t(w.P), t(w.dt), t(w.h), t(w.J)
+    spin = []
+    for _ in range(SPINUP_CALLS):
+        t0 = time.perf_counter()
+        x, h, _, steps = solver(x, T, P, dt, h, J=J)
+        spin.append({"s": round(time.perf_counter() - t0, 3), "steps_mean": float(steps.mean())})
+    check_inputs(dev, tab.ns, x, T, P, dt, h, 1e-3, 1e-25, 4000)
+    tries = torch.zeros(3, dtype=torch.int64, device=dev)
+    lib = abi.library()
+    lib.mx_set_try_counter(solver._handle, tries.data_ptr())
+    out = None
+    for _ in range(args.warmup):
+        out = solver.launch_raw(x, T, P, dt, h, rtol=1e-3, atol=1e-25, max_steps=4000, J=J, out=out)
+    torch.cuda.synchronize(dev)
+    tries.zero_()
+    stream = torch.cuda.current_stream(dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with Clocks(local) as clocks:
+        e_all0 = torch.cuda.Event(enable_timing=True)
+        e_all1 = torch.cuda.Event(enable_timing=True)
+        e_all0.record(stream)
+        for k in range(args.steps):
+            starts[k].record(stream)
+            out = solver.launch_raw(x, T, P, dt, h, rtol=1e-3, atol=1e-25, max_steps=4000, J=J, out=out)
+            ends[k].record(stream)
+        e_all1.record(stream)
+        torch.cuda.synchronize(dev)
+    total_ms = e_all0.elapsed_time(e_all1)
+    if world > 1:
+        m = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        total_ms = float(m.item())
+        dist.barrier()
+    ms = total_ms / args.steps
+    counts = solver.count.cpu().tolist()
+    nt = tries.cpu().tolist()
+    steps_mean = float(out["steps"].mean())
+    value = world * B / (ms * 1e-3)
+    # roofline: algorithmic FP64 work of the call kernel per launch / its time (events on the launching stream)
+    f = tab.flops
+    fresh, retry = nt[0] - nt[1], nt[1]
+    flop_step = (fresh * f["fresh_try"] + retry * f["retry"] + B * f["rates"]) / args.steps
+    peak = ctypes_probe(lib, local)
+    achieved = flop_step / (ms * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded 69-species network and column grid; the VULCAN networks are absent)",
+        "config": {"workload": f"{NETWORK}: call {SPINUP_CALLS + 1} of 300 s calls on a {LEVELS}-level column grid",
+                   "cells_per_gpu": B, "species": tab.ns, "reactions": tab.nr, "photolysis": tab.nj,
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
+                   "accepted_steps_mean": steps_mean, "tries_per_cell": nt[0] / args.steps / B,
+                   "retries_per_cell": nt[1] / args.steps / B, "recovery_tries": nt[2] / args.steps,
+                   "counts": dict(zip(["queue", *abi_counts()], counts)), "spinup": spin, "layout": solver.info},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak / 1e3, "unit": "TFLOP/s",
+                     "frac": achieved / (peak / 1e3) if peak else None, "traffic": None,
+                     "peak_source": "measured in-process: FP64 fma chains on every SM (mx_probe_fp64)",
+                     "flops_per_step": flop_step},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clocks.summary(),
+    }  # fmt: skip
+    if not args.no_e2e:
+        line["e2e"] = e2e(solver, x, h, w, dev, args)
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(tab, x, h, w, args)
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def abi_counts():
+    from maxichem_b200.constants import COUNTS
+
+    return [*COUNTS, "recovery_queue"]
+
+
+def ctypes_probe(lib, device: int) -> float:
+    import ctypes
+
+    g = ctypes.c_double()
+    lib.mx_probe_fp64(device, 20000, ctypes.byref(g))
+    return g.value
+
+
+def e2e(solver, x, h, w, dev, args) -> dict:
+    """The same call through the public API from pinned host buffers: H2D, call (with its count read-back), D2H."""
+    import torch
+
+    pin = lambda a: torch.as_tensor(a, dtype=torch.float64).pin_memory()
+    hx, hT, hP, hdt, hh, hJ = (pin(a) for a in (x.cpu(), w.T, w.P, w.dt, h.cpu(), w.J))
+    ox, oh, ost = (torch.empty_like(a).pin_memory() for a in (hx, hh, hh))
+    odone = torch.empty(hh.shape, dtype=torch.bool).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        d = [a.to(dev, non_blocking=True) for a in (hx, hT, hP, hdt, hh, hJ)]
+        r = solver(d[0], d[1], d[2], d[3], d[4], J=d[5])
+        ox.copy_(r.x, non_blocking=True)
+        oh.copy_(r.h, non_blocking=True)
+        odone.copy_(r.done, non_blocking=True)
+        ost.copy_(r.steps, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    h2d = sum(a.numel() * a.element_size() for a in (hx, hT, hP, hdt, hh, hJ))
+    d2h = sum(a.numel() * a.element_size() for a in (ox, oh, odone, ost))
+    return {"value": hx.shape[0] / (ms * 1e-3), "unit": "cells/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms}  # fmt: skip
+
+
+def cpu_baseline(tab, x, h, w, args) -> dict:
+    """The oracle on the host's cores on a bounded sample of the same call (the first cells of the batch)."""
+    import oracle
+
+    n = min(args.cpu_sample, x.shape[0])
+    xs, hs = x[:n].cpu().numpy(), h[:n].cpu().numpy()
+    ref = oracle.Oracle(tab)
+    t0 = time.perf_counter()
+    ref.call(xs, w.T[:n], w.P[:n], w.dt[:n], hs, J=w.J[:n])
+    dt = time.perf_counter() - t0
+    cores = oracle.threads()
+    return {"value": n / dt, "unit": "cells/s", "cores": cores, "kind": "port",
+            "sample": f"first {n} cells of the timed call, {dt:.1f} s on {cores} host threads"}  # fmt: skip
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,152 @@
+/*
+ * maxichem_b200: the per-call chemistry solve of imalsky/maxichem as a C-ABI library for NVIDIA B200 (sm_100a).
+ *
+ * One call advances B independent 0-D gas cells by their own dt with Rodas3 (order 3, L-stable), the exact
+ * mass-action Jacobian, adaptive steps, and a guard/recovery pass; it is the device-side body of the reference's
+ * CudaSolver call (maxichem/kincuda.py:230-320). Python's CudaSolver (maxichem_b200/solver.py) rebuilds the
+ * reference's Python surface on top of these entry points through ctypes.
+ *
+ * Conventions: all array arguments of mx_call are DEVICE pointers on the solver's device, row-major, float64 unless
+ * stated; nothing is allocated per call; errors come back as a nonzero status and a message in err (never an
+ * exception across the ABI). Inputs and outputs must not alias. Calls on one solver run one at a time on the given
+ * stream (its scratch, queues and list are shared), as the reference's do (maxichem/kincuda.py:114-116).
+ */
+#ifndef MAXICHEM_B200_H
+#define MAXICHEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Settings, with the reference's values (maxichem/_constants.py:12-78); maxichem_b200/constants.py holds the same. */
+#define MX_T_MIN 300.0
+#define MX_T_MAX 3000.0
+#define MX_X_SUM_TOL 1e-10
+#define MX_DRIFT 1e-6
+#define MX_REC_STEPS 10
+#define MX_H_MIN 1e-12
+#define MX_CALL_END (1.0 - 1e-14)
+#define MX_STEP_SAFETY 0.9
+#define MX_ERR_FLOOR 1e-10
+#define MX_FAC_NONFINITE 0.1
+#define MX_FACACC 0.2
+#define MX_FACREJ 0.2
+#define MX_FACMAX 20.0
+#define MX_FAC_AFTER_REJECT 0.5
+#define MX_SECMIN 1e-4
+#define MX_SECANT_MIN_ORDER 0.05
+#define MX_SECANT_MAX_ORDER 3.0
+#define MX_SECANT_TARGET 0.5
+#define MX_PIVTAU 0.1
+#define MX_ELEMENT_PIVOT_MIN 1e-10
+#define MX_REC_RETRIES 3
+#define MX_REC_RETRY_SPLIT 0.5
+#define MX_GMAX 1e-3
+#define MX_KB 1.380649e-16
+#define MX_P0 1.0e6
+#define MX_NASA_SPLIT_T 1000.0
+#define MX_K_COLL 1e-9
+#define MX_MAX_SPECIES 254
+#define MX_MAX_ELEMENTS 8
+
+/* Count slots of the device count array (maxichem/_constants.py:100-113). */
+enum {
+  MX_COUNT_QUEUE = 0,
+  MX_COUNT_BAD_INPUT,
+  MX_COUNT_COLD,
+  MX_COUNT_HOT,
+  MX_COUNT_NONFINITE,
+  MX_COUNT_UNFINISHED,
+  MX_COUNT_DRIFT,
+  MX_COUNT_RECOMPUTED,
+  MX_COUNT_RECOVERED,
+  MX_COUNT_STILL_FAILED,
+  MX_COUNT_NONFINITE_H,
+  MX_COUNT_RECOVERY_QUEUE,
+  MX_COUNT_SLOTS
+};
+
+/* Status codes (maxichem/kernels/common.cuh:260-262). */
+enum { MX_STATUS_OK = 0, MX_REFUSED_COLD = 1, MX_REFUSED_BAD_INPUT = 2, MX_REFUSED_HOT = 3 };
+
+/* Return codes of the entry points. */
+enum { MX_OK = 0, MX_ERR_ARGUMENT = 1, MX_ERR_CUDA = 2, MX_ERR_NETWORK = 3, MX_ERR_CLOSED = 4 };
+
+/*
+ * A network's tables in host memory, as maxichem_b200/tables.py builds them. Rows are in elimination order (the
+ * reference's minimum-degree order, maxichem/_tables.py:35-50) except atoms, which is in the network's species order.
+ */
+typedef struct mx_network {
+  int32_t ns, nr, nrt, nj, nel;  /* species, reactions (thermal then photolysis), thermal, photolysis, elements */
+  int32_t n_entries;             /* Jacobian entries */
+  int32_t has_troe, has_eff;
+  const int32_t* perm;           /* [ns] network species of elimination row i */
+  const uint8_t* rx;             /* [nr][6] reactants 0-2, products 3-5 (elimination rows, padding ns) */
+  const double* rc;              /* [nr][14] ln A0 B0 C0, ln A1 B1 C1, ln Ai Bi Ci, Troe a T3 T1 T2, efficiency */
+  const int32_t* rf;             /* [nr] law flags */
+  const double* nasa;            /* [2][ns][9] NASA-9 ranges below and above MX_NASA_SPLIT_T */
+  const double* atoms;           /* [ns][nel] network species order */
+  const int32_t* sv_ptr;         /* [ns + 1] */
+  const uint32_t* sv_term;       /* reaction | coefficient code << 16 */
+  const int32_t* jac_ptr;        /* [n_entries + 1] */
+  const uint32_t* jac_entry;     /* row << 16 | column */
+  const uint32_t* jac_term;      /* rate index | code << 12 | a << 16 | b << 24 */
+  const uint8_t* fill;           /* [ns][ns] pattern of L + U (the oracle's sparse factorisation) */
+} mx_network;
+
+typedef struct mx_solver mx_solver;
+
+/*
+ * Build a solver for one network on one CUDA device (replaces CudaSolver.__init__/_setup, maxichem/kincuda.py:130-227):
+ * copies the tables to the device, sizes the persistent launches and allocates the solver-owned scratch.
+ * drift: the guard's element-drift allowance (finite, >= 0).
+ */
+int mx_create(const mx_network* net, double drift, int device, mx_solver** out, char* err, size_t errlen);
+
+/*
+ * One call (replaces CudaSolver.launch's three launches, maxichem/kincuda.py:279-317, without the host read of the
+ * counts): screening, rates, Rodas3 steps and the guard in one persistent kernel, then the recovery of the cells the
+ * guard listed, then total += count. No host synchronisation.
+ * Inputs:  x [B][ns], T, P, dt, h_in [B], J [B][nj] (NULL when nj == 0).
+ * Outputs: x_out [B][ns], h_out [B], done [B] (int32 0/1), steps [B], flag [B] (int32 0/1/2), status [B] (int32).
+ * count: int32[MX_COUNT_SLOTS], zeroed and filled by the call; total: int64[MX_COUNT_SLOTS], incremented.
+ * stream: a cudaStream_t (NULL: the legacy default stream).
+ */
+int mx_call(mx_solver* s, const double* x, const double* T, const double* P, const double* dt, const double* h_in,
+            const double* J, int64_t B, double rtol, double atol, int32_t max_steps, double* x_out, double* h_out,
+            int32_t* done, double* steps, int32_t* flag, int32_t* status, int32_t* count, int64_t* total,
+            void* stream, char* err, size_t errlen);
+
+/* The guard alone on given states (replaces a launch of the reference's guard kernel, maxichem/kernels/guard.cuh:114):
+ * counts refused cells from status, checks and corrects the others in x_out, writes flag 0/1 and the recompute list
+ * count. Device pointers; used by tests of the guard's thresholds. */
+int mx_guard(mx_solver* s, const double* x, double* x_out, const int32_t* done, const double* steps,
+             const int32_t* status, int64_t B, double atol, int32_t* flag, int32_t* count, void* stream, char* err,
+             size_t errlen);
+
+/* Launch layout of the solver (cells per CTA, warps per cell, CTAs per SM, shared bytes), for reports. */
+int mx_info(const mx_solver* s, int32_t* values, int32_t n);
+
+/* Register a device int64[3] that later calls of this solver add their tries to: [0] the call kernel's tries, [1] those
+ * that followed a rejection, [2] the recovery's tries (NULL stops counting). No counterpart in the reference: it
+ * feeds the measured roofline (algorithmic FLOPs per try are a property of the network's tables). */
+int mx_set_try_counter(mx_solver* s, int64_t* tries);
+
+/* FP64 fused multiply-add throughput of a device in GFLOP/s, from independent fma chains on every SM (synchronises
+ * the device). No counterpart in the reference: the roofline's FP64 denominator, which the driver-measured peaks
+ * file does not hold. */
+int mx_probe_fp64(int device, int64_t iters, double* gflops);
+
+/* Release the solver's device memory. Safe on NULL. */
+int mx_destroy(mx_solver* s);
+
+/* The library's build identity (architecture and version), a static string. */
+const char* mx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

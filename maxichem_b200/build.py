@@ -1,0 +1,41 @@
+"""Build the CUDA library ``_build/libmaxichem_b200.so`` for sm_100a with nvcc (in-tree, no JIT cache)."""
+
+from __future__ import annotations
+
+import os
+import subprocess
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+SOURCES = [PACKAGE / "csrc" / "maxichem_b200.cu"]
+HEADERS = [PACKAGE / "csrc" / "device.cuh", PACKAGE.parent / "include" / "maxichem_b200.h"]
+OUTPUT = PACKAGE / "_build" / "libmaxichem_b200.so"
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    "-fmad=false",  # every fused multiply-add in the kernels is an explicit fma(): the same bits as the oracle's
+    "-Xptxas", "-v",
+    "-Xcompiler", "-fPIC", "-shared",
+]  # fmt: skip
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile the library if a source is newer than it (or force); return its path."""
+    OUTPUT.parent.mkdir(exist_ok=True)
+    newest = max(p.stat().st_mtime for p in SOURCES + HEADERS)
+    if force or not OUTPUT.exists() or OUTPUT.stat().st_mtime < newest:
+        tmp = OUTPUT.with_suffix(".tmp.so")
+        cmd = [NVCC, *FLAGS, *map(str, SOURCES), "-o", str(tmp)]
+        out = subprocess.run(cmd, capture_output=True, text=True)
+        if out.returncode != 0:
+            raise RuntimeError(f"nvcc failed:\n{out.stderr}")
+        (OUTPUT.parent / "ptxas.log").write_text(out.stderr)
+        if verbose:
+            print(out.stderr)
+        tmp.replace(OUTPUT)
+    return OUTPUT
+
+
+if __name__ == "__main__":
+    build(force=True, verbose=True)

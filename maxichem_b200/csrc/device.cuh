@@ -1,0 +1,561 @@
+// Device arithmetic of the per-call chemistry solve: rates, right-hand side, Jacobian, dense LU and solves,
+// Rodas3 stages, step control and the guard. One CTA steps one cell at a time; its W warps share the cell's arrays in
+// shared memory. Every sum that reaches the state has a fixed order (ascending index, or the 32-lane butterfly), so
+// a cell's result does not depend on the batch, its order, or the launch shape.
+//
+// Arithmetic follows imalsky/maxichem maxichem/kernels/common.cuh, call.cuh, guard.cuh and recover.cuh (cited per
+// function). The library is built with -fmad=false: every fused multiply-add is an explicit fma().
+#pragma once
+#include <cstdint>
+
+#include "../../include/maxichem_b200.h"
+
+namespace mx {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr double GAMMA = 0.5;            // Rodas3's diagonal coefficient (Sandu et al. 1997)
+constexpr double RODAS_C21 = 4.0;        // stage coupling C_21
+constexpr double RODAS_C43 = 8.0 / 3.0;  // stage coupling, -C_43
+constexpr double TROE_C0 = 0.4, TROE_C1 = 0.67, TROE_N0 = 0.75, TROE_N1 = 1.27, TROE_D = 0.14;  // Venot et al. 2012
+constexpr int FL_FALLOFF = 1, FL_SECOND_K0 = 2, FL_THREE_BODY = 4, FL_TROE = 64, FL_EFF = 128, FL_VM11 = 512;
+constexpr int GUARD_NONFINITE = 4, GUARD_UNFINISHED = 8, GUARD_DRIFT = 16;
+constexpr int PANEL = 8;  // pivots per block of the blocked LU
+
+// A network's tables on the device, and the per-CTA shared-memory layout (offsets in doubles).
+struct Net {
+  int ns, nr, nrt, nj, nel, n_entries;
+  const int* perm;
+  const uint64_t* rx8;  // 8 bytes per reaction: reactants 0-2, products 3-5, padding
+  const double* rc;
+  const int* rf;
+  const double* nasa;
+  const double* atoms;
+  const int* sv_ptr;
+  const uint32_t* sv_term;
+  const int* jac_ptr;
+  const uint32_t* jac_entry;
+  const uint32_t* jac_term;
+  double etot, drift;
+  // shared-memory layout
+  int ld, oA, oK, oV, on, oN, oY, oF, oU, oK1, oK2, oK3, oK4, oD, oRed, oInts, doubles;
+};
+
+struct CallArgs {
+  const double *x, *T, *P, *dt, *h_in, *J;
+  int B;
+  double rtol, atol;
+  int max_steps;
+  double *x_out, *h_out;
+  int* done;
+  double* steps;
+  int *flag, *status, *count, *list;
+  unsigned long long* tries;  // nullable: [0] tries, [1] tries after a rejection, [2] recovery tries
+};
+
+// Pointers into one CTA's shared memory.
+struct Cell {
+  double *A, *kf, *kr, *v, *n, *N, *Y, *F, *U, *K1, *K2, *K3, *K4, *dinv, *red;
+  int* ints;
+};
+
+__device__ __forceinline__ Cell cell_arrays(const Net& net, double* smem) {
+  Cell c;
+  c.A = smem + net.oA;
+  c.kf = smem + net.oK;
+  c.kr = c.kf + net.nr;
+  c.v = smem + net.oV;
+  c.n = smem + net.on;
+  c.N = smem + net.oN;
+  c.Y = smem + net.oY;
+  c.F = smem + net.oF;
+  c.U = smem + net.oU;
+  c.K1 = smem + net.oK1;
+  c.K2 = smem + net.oK2;
+  c.K3 = smem + net.oK3;
+  c.K4 = smem + net.oK4;
+  c.dinv = smem + net.oD;
+  c.red = smem + net.oRed;
+  c.ints = (int*)(smem + net.oInts);
+  return c;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+  return v;
+}
+
+// sum of y[0..n) as a warp forms it: lane l adds y[l], y[l + 32], ... then the butterfly (every lane returns it).
+__device__ __forceinline__ double lane_sum(const double* y, int n, int lane) {
+  double p = 0.0;
+  for (int i = lane; i < n; i += 32) p += y[i];
+  return warp_sum(p);
+}
+
+__device__ __forceinline__ double code_coefficient(unsigned c) {
+  return (c & 2u) ? ((c & 1u) ? -2.0 : 2.0) : ((c & 1u) ? -1.0 : 1.0);
+}
+
+// ---- rates (common.cuh:136-242) ----
+
+__device__ __forceinline__ double law(const double* __restrict__ q, int fl, double Tc, double lT, double iT,
+                                      double nd) {
+  double k = exp(q[0] + q[1] * lT - q[2] * iT);
+  if (fl & FL_SECOND_K0) k += exp(q[3] + q[4] * lT - q[5] * iT);
+  if (fl & FL_FALLOFF) {
+    const double pr = k * nd / exp(q[6] + q[7] * lT - q[8] * iT);
+    k = k > 0.0 ? k / (1.0 + pr) : 0.0;
+    if ((fl & FL_TROE) && k > 0.0) {
+      const double fc = log10((1.0 - q[9]) * exp(-Tc / q[10]) + q[9] * exp(-Tc / q[11]) + exp(-q[12] / Tc));
+      const double x = (fl & FL_VM11) ? log10(pr) : log10(pr) - TROE_C0 - TROE_C1 * fc;
+      // at Pr = 0 the standard ratio tends to -1 / d, so F to Fc^(d^2 / (1 + d^2)); the VM11 one to -inf, F to 1
+      const double y = (fl & FL_VM11) ? x / (TROE_N0 - TROE_N1 * fc)
+                                      : (isfinite(x) ? x / (TROE_N0 - TROE_N1 * fc - TROE_D * x) : -1.0 / TROE_D);
+      k *= exp10(fc / (1.0 + y * y));
+    }
+  }
+  if (fl & FL_EFF) k *= q[13];
+  return k;
+}
+
+__device__ __forceinline__ double bimolecular_rate(int molecules, bool three_body, double k, double nd) {
+  return molecules >= 2 ? k * (molecules == 3 ? nd : 1.0) : (three_body ? k / nd : 0.0);
+}
+
+__device__ __forceinline__ double gibbs_rt(const double* __restrict__ a, double Tc, double lT, double iT) {
+  const double T2 = Tc * Tc, T3 = T2 * Tc, T4 = T3 * Tc;
+  const double h = -a[0] * iT * iT + a[1] * lT * iT + a[2] + a[3] * Tc / 2 + a[4] * T2 / 3 + a[5] * T3 / 4 +
+                   a[6] * T4 / 5 + a[7] * iT;
+  const double s = -a[0] * iT * iT / 2 - a[1] * iT + a[2] * lT + a[3] * Tc + a[4] * T2 / 2 + a[5] * T3 / 3 +
+                   a[6] * T4 / 4 + a[8];
+  return h - s;
+}
+
+// kf, kr of one cell (cell_rates, common.cuh:222-242); g (ns + 1 doubles) is scratch. Two barriers.
+__device__ void cell_rates(const Net& net, const Cell& c, double Tc, double nd, const double* __restrict__ Jc,
+                           int tid, int nt) {
+  const double lT = log(Tc), iT = 1.0 / Tc, lKT = log(MX_KB * Tc / MX_P0);
+  double* g = c.v;
+  const double* cf = net.nasa + (Tc < MX_NASA_SPLIT_T ? 0 : net.ns * 9);
+  for (int i = tid; i < net.ns; i += nt) g[i] = gibbs_rt(cf + 9 * i, Tc, lT, iT);
+  if (tid == 0) g[net.ns] = 0.0;
+  __syncthreads();
+  for (int r = tid; r < net.nr; r += nt) {
+    if (r >= net.nrt) {
+      c.kf[r] = Jc[r - net.nrt];
+      c.kr[r] = 0.0;
+      continue;
+    }
+    const int fl = __ldg(net.rf + r);
+    const uint64_t w = __ldg(net.rx8 + r);
+    const int x0 = w & 255, x1 = (w >> 8) & 255, x2 = (w >> 16) & 255;
+    const int x3 = (w >> 24) & 255, x4 = (w >> 32) & 255, x5 = (w >> 40) & 255;
+    const double k = law(net.rc + 14 * r, fl, Tc, lT, iT, nd);
+    const double dg = g[x3] + g[x4] + g[x5] - g[x0] - g[x1] - g[x2];
+    const double c3 = (fl & FL_THREE_BODY) ? nd : 1.0;
+    const double dmu = (double)(((fl >> 3) & 7) - 4);
+    double kf = k * c3, kr = (k * exp(dg + dmu * lKT)) * c3;
+    const int mf = (fl >> 10) & 3, mr = (fl >> 12) & 3;
+    const bool tb = (fl & FL_THREE_BODY) != 0;
+    const double q = fmax(bimolecular_rate(mf, tb, kf, nd), bimolecular_rate(mr, tb, kr, nd));
+    if (q > MX_K_COLL) {
+      const double cc = MX_K_COLL / q;
+      kf *= cc;
+      kr *= cc;
+    }
+    c.kf[r] = kf;
+    c.kr[r] = kr;
+  }
+  __syncthreads();
+}
+
+// ---- right-hand side (rhs, common.cuh:282-353) ----
+
+// F = (ntot / nd) S v(n) at Y, u0 = S v / nd into U when u0; n = nd Y / ntot. Returns ntot. Three barriers.
+__device__ double rhs(const Net& net, const Cell& c, const double* Y, bool u0, double nd, int tid, int nt) {
+  const int lane = tid & 31, ns = net.ns;
+  const double ntot = lane_sum(Y, ns, lane), xf = nd / ntot, ixf = ntot / nd;
+  for (int i = tid; i < ns; i += nt) c.n[i] = Y[i] * xf;
+  if (tid == 0) c.n[ns] = 1.0;
+  __syncthreads();
+  const double* n = c.n;
+  for (int r = tid; r < net.nr; r += nt) {
+    const uint64_t w = __ldg(net.rx8 + r);
+    const double a = c.kf[r] * n[w & 255] * n[(w >> 8) & 255] * n[(w >> 16) & 255];
+    const double b = c.kr[r] * n[(w >> 24) & 255] * n[(w >> 32) & 255] * n[(w >> 40) & 255];
+    c.v[r] = a - b;
+  }
+  __syncthreads();
+  for (int i = tid; i < ns; i += nt) {
+    double s = 0.0;
+    const int t1 = __ldg(net.sv_ptr + i + 1);
+    for (int t = __ldg(net.sv_ptr + i); t < t1; t++) {
+      const unsigned w = __ldg(net.sv_term + t);
+      s = fma(code_coefficient(w >> 16), c.v[w & 0xffffu], s);
+    }
+    c.F[i] = s * ixf;
+    if (u0) c.U[i] = s / nd;
+  }
+  __syncthreads();
+  return ntot;
+}
+
+// A = -Jn (dense, row stride ld), then U = u0 + (-Jn N) / ntot (call.cuh:61-79, jacobian_times_x). Three barriers.
+__device__ void jacobian_w(const Net& net, const Cell& c, double ntot, int tid, int nt) {
+  const int ns = net.ns, ld = net.ld;
+  for (int i = tid; i < ns * ld; i += nt) c.A[i] = 0.0;
+  __syncthreads();
+  for (int e = tid; e < net.n_entries; e += nt) {
+    double acc = 0.0;
+    const int t1 = __ldg(net.jac_ptr + e + 1);
+    for (int t = __ldg(net.jac_ptr + e); t < t1; t++) {
+      const unsigned w = __ldg(net.jac_term + t);
+      const double pr = c.kf[w & 0xfffu] * c.n[(w >> 16) & 255u] * c.n[w >> 24];
+      acc = fma(code_coefficient(w >> 12), pr, acc);
+    }
+    const unsigned pq = __ldg(net.jac_entry + e);
+    c.A[(int)(pq >> 16) * ld + (int)(pq & 0xffffu)] = -acc;
+  }
+  __syncthreads();
+  for (int i = tid; i < ns; i += nt) {
+    const double* a = c.A + i * ld;
+    double acc = 0.0;
+    for (int j = 0; j < ns; j++) acc = fma(a[j], c.N[j], acc);
+    c.U[i] = c.U[i] + acc / ntot;
+  }
+  __syncthreads();
+}
+
+// ---- dense LU without exchanges, blocked (PANEL pivots at a time) ----
+// Every entry receives its updates A_ij <- fma(-l_ik, A_kj, A_ij) in ascending k, l_ik = A_ik / A_kk taken as
+// A_ik * (1 / A_kk): the order and the operations of the right-looking LU, so the bits of the sparse factorisation
+// on the fill pattern (call.cuh:81-112) for finite data.
+__device__ void lu_factor(const Net& net, double* A, double* dinv, int tid, int nt) {
+  const int ns = net.ns, ld = net.ld;
+  for (int kb = 0; kb < ns; kb += PANEL) {
+    const int ke = min(kb + PANEL, ns), nb = ke - kb;
+    for (int k = kb; k < ke; k++) {  // the panel: columns kb..ke-1
+      const double d = 1.0 / A[k * ld + k];
+      if (tid == 0) dinv[k] = d;
+      for (int i = k + 1 + tid; i < ns; i += nt) {
+        double* ai = A + i * ld;
+        const double l = ai[k] * d;
+        ai[k] = l;
+        for (int j = k + 1; j < ke; j++) ai[j] = fma(-l, A[k * ld + j], ai[j]);
+      }
+      __syncthreads();
+    }
+    if (ke == ns) break;
+    // the block's pivot rows beyond the panel: row kb + s takes pivots kb .. kb + s - 1
+    for (int j = ke + tid; j < ns; j += nt) {
+      for (int s = 1; s < nb; s++) {
+        double a = A[(kb + s) * ld + j];
+        for (int t = 0; t < s; t++) a = fma(-A[(kb + s) * ld + kb + t], A[(kb + t) * ld + j], a);
+        A[(kb + s) * ld + j] = a;
+      }
+    }
+    __syncthreads();
+    // the trailing matrix: rank-nb update, one row per thread
+    for (int i = ke + tid; i < ns; i += nt) {
+      double l[PANEL];
+      double* ai = A + i * ld;
+#pragma unroll
+      for (int t = 0; t < PANEL; t++) l[t] = t < nb ? ai[kb + t] : 0.0;
+      for (int j = ke; j < ns; j++) {
+        double a = ai[j];
+#pragma unroll
+        for (int t = 0; t < PANEL; t++)
+          if (t < nb) a = fma(-l[t], A[(kb + t) * ld + j], a);
+        ai[j] = a;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// value a[p] for p = idx (R known at compile time: no local memory)
+template <int R>
+__device__ __forceinline__ double pick(const double (&a)[R], int idx) {
+  double v = a[0];
+#pragma unroll
+  for (int p = 1; p < R; p++)
+    if (idx == p) v = a[p];
+  return v;
+}
+
+// y <- M0^-1 y on one warp for NV vectors (1 or 2) with the factors of lu_factor: lane l holds rows l + 32 p.
+// Forward unit L in ascending k, U in descending k with x_k = a_k / U_kk (msolve, common.cuh:504-522).
+template <int R, int NV>
+__device__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1, int lane) {
+  const int ns = net.ns, ld = net.ld;
+  double a[NV][R], d[R];
+#pragma unroll
+  for (int p = 0; p < R; p++) {
+    const int i = lane + 32 * p;
+    d[p] = i < ns ? dinv[i] : 0.0;
+    a[0][p] = i < ns ? y0[i] : 0.0;
+    if (NV == 2) a[NV - 1][p] = i < ns ? y1[i] : 0.0;
+  }
+  for (int k = 0; k < ns - 1; k++) {
+    const int src = k & 31, kp = k >> 5;
+    const double yk0 = __shfl_sync(FULL, pick<R>(a[0], kp), src);
+    const double yk1 = NV == 2 ? __shfl_sync(FULL, pick<R>(a[NV - 1], kp), src) : 0.0;
+#pragma unroll
+    for (int p = 0; p < R; p++) {
+      const int i = lane + 32 * p;
+      if (32 * p + 31 > k && i > k && i < ns) {
+        const double m = A[i * ld + k];
+        a[0][p] = fma(-m, yk0, a[0][p]);
+        if (NV == 2) a[NV - 1][p] = fma(-m, yk1, a[NV - 1][p]);
+      }
+    }
+  }
+  for (int k = ns - 1; k > 0; k--) {
+    const int src = k & 31, kp = k >> 5;
+    const double z0 = __shfl_sync(FULL, pick<R>(a[0], kp) * pick<R>(d, kp), src);
+    const double z1 = NV == 2 ? __shfl_sync(FULL, pick<R>(a[NV - 1], kp) * pick<R>(d, kp), src) : 0.0;
+#pragma unroll
+    for (int p = 0; p < R; p++) {
+      const int i = lane + 32 * p;
+      if (32 * p < k && i < k) {
+        const double m = A[i * ld + k];
+        a[0][p] = fma(-m, z0, a[0][p]);
+        if (NV == 2) a[NV - 1][p] = fma(-m, z1, a[NV - 1][p]);
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int p = 0; p < R; p++) {
+    const int i = lane + 32 * p;
+    if (i < ns) {
+      y0[i] = a[0][p] * d[p];
+      if (NV == 2) y1[i] = a[NV - 1][p] * d[p];
+    }
+  }
+  __syncwarp();
+}
+
+// y <- y + c0 (sum y) u on one warp (sherman_morrison_update, common.cuh:542-557)
+__device__ __forceinline__ void sherman(const Net& net, double* y, const double* u, double c0, int lane) {
+  const double s = lane_sum(y, net.ns, lane) * c0;
+  for (int i = lane; i < net.ns; i += 32) y[i] = fma(s, u[i], y[i]);
+  __syncwarp();
+}
+
+// ---- the recovery's dense LU with threshold partial pivoting (recover.cuh:7-82), on one warp ----
+
+__device__ void dense_lu_pivot(const Net& net, double* A, double* dinv, int* pr, int lane) {
+  const int ns = net.ns, ld = net.ld;
+  for (int i = lane; i < ns; i += 32) pr[i] = i;
+  __syncwarp();
+  for (int k = 0; k < ns; k++) {
+    double best = -1.0;
+    int bi = ns;
+    for (int i = k + lane; i < ns; i += 32) {
+      const double a = fabs(A[i * ld + k]);
+      if (a > best) {
+        best = a;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(FULL, best, o);
+      const int oi = __shfl_xor_sync(FULL, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    const bool exchange = bi != ns && bi != k && !(fabs(A[k * ld + k]) >= MX_PIVTAU * best);
+    __syncwarp();
+    if (exchange) {
+      for (int j = lane; j < ns; j += 32) {
+        const double a = A[k * ld + j];
+        A[k * ld + j] = A[bi * ld + j];
+        A[bi * ld + j] = a;
+      }
+      if (lane == 0) {
+        const int t = pr[k];
+        pr[k] = pr[bi];
+        pr[bi] = t;
+      }
+    }
+    __syncwarp();
+    const double dk = 1.0 / A[k * ld + k];
+    if (lane == 0) dinv[k] = dk;
+    for (int i = k + 1 + lane; i < ns; i += 32) {
+      const double l = A[i * ld + k] * dk;
+      A[i * ld + k] = l;
+      for (int j = k + 1; j < ns; j++) A[i * ld + j] = fma(-l, A[k * ld + j], A[i * ld + j]);
+    }
+    __syncwarp();
+  }
+}
+
+template <int R>
+__device__ void dense_solve(const Net& net, const double* A, const double* dinv, const int* pr, double* y, int lane) {
+  const int ns = net.ns, ld = net.ld;
+  double a[R], d[R];
+#pragma unroll
+  for (int p = 0; p < R; p++) {
+    const int i = lane + 32 * p;
+    a[p] = i < ns ? y[pr[i]] : 0.0;
+    d[p] = i < ns ? dinv[i] : 0.0;
+  }
+  for (int k = 0; k < ns - 1; k++) {
+    const double yk = __shfl_sync(FULL, pick<R>(a, k >> 5), k & 31);
+#pragma unroll
+    for (int p = 0; p < R; p++) {
+      const int i = lane + 32 * p;
+      if (i > k && i < ns) a[p] = fma(-A[i * ld + k], yk, a[p]);
+    }
+  }
+  for (int k = ns - 1; k > 0; k--) {
+    const double z = __shfl_sync(FULL, pick<R>(a, k >> 5) * pick<R>(d, k >> 5), k & 31);
+#pragma unroll
+    for (int p = 0; p < R; p++) {
+      const int i = lane + 32 * p;
+      if (i < k) a[p] = fma(-A[i * ld + k], z, a[p]);
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int p = 0; p < R; p++) {
+    const int i = lane + 32 * p;
+    if (i < ns) y[i] = a[p] * d[p];
+  }
+  __syncwarp();
+}
+
+// ---- step control (common.cuh:90-133) ----
+
+struct StepState {
+  double h, t, nok, pen, pha;
+  bool prej;
+};
+
+__device__ __forceinline__ double step_factor(double en, bool ok, bool prej, double pen, double pha, double ha) {
+  const bool efin = isfinite(en);
+  double fac = efin ? MX_STEP_SAFETY / cbrt(fmax(en, MX_ERR_FLOOR)) : MX_FAC_NONFINITE;
+  fac = fmin(fmax(fac, ok ? MX_FACACC : MX_FACREJ), MX_FACMAX);
+  if (!ok && efin && prej && en > 1.0 && pen > 1.0 && pha > ha) {
+    const double pe = log(pen / en) / log(pha / ha);
+    fac = pe > MX_SECANT_MIN_ORDER
+              ? fmax(pow(MX_SECANT_TARGET / en, 1.0 / fmin(pe, MX_SECANT_MAX_ORDER)), MX_SECMIN)
+              : MX_SECMIN;
+  }
+  if (!ok) fac = fmin(fac, MX_FAC_AFTER_REJECT);
+  return fac;
+}
+
+// err of a try on warp 0 (try_error, common.cuh:570-590): Y = N + 2 K1 + K3 + K4; writes en and ok to red[0..1].
+__device__ void try_error(const Net& net, const Cell& c, bool first, double rtol, double atol, int lane) {
+  double e2 = 0.0, em = 0.0;
+  bool nn = true;
+  for (int i = lane; i < net.ns; i += 32) {
+    const double y = c.N[i] + 2.0 * c.K1[i] + c.K3[i] + c.K4[i];
+    c.Y[i] = y;
+    const double sc = fma(rtol, fmax(fabs(c.N[i]), fabs(y)), atol);
+    const double q = c.K4[i] / sc;
+    e2 = fma(q, q, e2);
+    em = fmax(em, fabs(q));
+    nn = nn && (y >= -atol);
+  }
+  const double er = sqrt(warp_sum(e2) / net.ns), emx = warp_max(em);
+  const double en = (first && isfinite(er)) ? fmax(er, emx) : er;
+  const bool ok = (en <= 1.0) && __all_sync(FULL, nn) && isfinite(en);
+  if (lane == 0) {
+    c.red[0] = en;
+    c.red[1] = ok ? 1.0 : 0.0;
+  }
+}
+
+// ---- the guard's test (guard.cuh:13-108), on one thread ----
+
+__device__ void element_multipliers(int ns, int nel, const double* q, const double* __restrict__ atoms,
+                                    const double* e0, const double* e1, double r, double* lam) {
+  double m[MX_MAX_ELEMENTS * MX_MAX_ELEMENTS], m0[MX_MAX_ELEMENTS], y[MX_MAX_ELEMENTS];
+  for (int e = 0; e < nel * nel; e++) m[e] = 0.0;
+  for (int i = 0; i < ns; i++) {
+    const double* ai = atoms + i * nel;
+    for (int e = 0; e < nel; e++) {
+      if (ai[e] == 0.0) continue;
+      for (int f = e; f < nel; f++)
+        if (ai[f] != 0.0) m[e * nel + f] = fma(ai[e] * ai[f], q[i], m[e * nel + f]);
+    }
+  }
+  for (int e = 0; e < nel; e++) {
+    m0[e] = m[e * nel + e];
+    y[e] = fma(e0[e], r, -e1[e]);
+  }
+  for (int k = 0; k < nel; k++) {
+    if (!(m[k * nel + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
+    for (int j = k + 1; j < nel; j++) {
+      const double l = m[k * nel + j] / m[k * nel + k];
+      for (int f = j; f < nel; f++) m[j * nel + f] = fma(-l, m[k * nel + f], m[j * nel + f]);
+      y[j] = fma(-l, y[k], y[j]);
+    }
+  }
+  for (int k = nel - 1; k >= 0; k--) {
+    lam[k] = 0.0;
+    if (!(m[k * nel + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
+    double b = y[k];
+    for (int f = k + 1; f < nel; f++) b = fma(-m[k * nel + f], lam[f], b);
+    lam[k] = b / m[k * nel + k];
+  }
+}
+
+// Guard bits of a stepped cell's result xo (network order) against its input x0; a passing result has its element
+// shares put back in place (check_cell).
+__device__ int check_cell(const Net& net, const double* __restrict__ x0, double* xo, int done, double nok,
+                          double atol) {
+  const int ns = net.ns, nel = net.nel;
+  double e0[MX_MAX_ELEMENTS], e1[MX_MAX_ELEMENTS], lam[MX_MAX_ELEMENTS];
+  for (int e = 0; e < nel; e++) e0[e] = e1[e] = 0.0;
+  bool xfin = true;
+  for (int i = 0; i < ns; i++) {
+    const double a = x0[i], b = xo[i];
+    xfin = xfin && isfinite(b);
+    for (int e = 0; e < nel; e++) {
+      const double at = __ldg(net.atoms + i * nel + e);
+      e0[e] = fma(at, a, e0[e]);
+      e1[e] = fma(at, b, e1[e]);
+    }
+  }
+  double s0 = 0.0, s1 = 0.0;
+  for (int e = 0; e < nel; e++) {
+    s0 += e0[e];
+    s1 += e1[e];
+  }
+  bool drift = false;
+  for (int e = 0; e < nel; e++)
+    drift = drift || fabs(e1[e] / s1 - e0[e] / s0) > net.drift * e0[e] / s0 + 2.0 * atol * nok * net.etot / s0;
+  const int c = (xfin ? 0 : GUARD_NONFINITE) | (done ? 0 : GUARD_UNFINISHED) | (drift ? GUARD_DRIFT : 0);
+  if (c) return c;
+  element_multipliers(ns, nel, xo, net.atoms, e0, e1, s1 / s0, lam);
+  double sum = 0.0;
+  for (int i = 0; i < ns; i++) {
+    double g = 1.0;
+    for (int e = 0; e < nel; e++) {
+      const double at = __ldg(net.atoms + i * nel + e);
+      if (at != 0.0) g = fma(lam[e], at, g);
+    }
+    g = fmin(fmax(g, 1.0 - MX_GMAX), 1.0 + MX_GMAX);
+    sum = fma(xo[i], g, sum);
+    xo[i] *= g;
+  }
+  if (!(isfinite(sum) && sum > 0.0)) return GUARD_NONFINITE;
+  const double is = 1.0 / sum;
+  for (int i = 0; i < ns; i++) xo[i] *= is;
+  return 0;
+}
+
+}  // namespace mx

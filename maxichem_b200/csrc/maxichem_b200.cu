@@ -1,0 +1,669 @@
+// The C-ABI library: the call, recovery and guard kernels for sm_100a, and the entry points of
+// include/maxichem_b200.h.
+//
+// Layout: one CTA of W warps steps one cell at a time, persistent over an atomic cell queue (call.cuh:174-176 of the
+// reference keeps the same queue), with the cell's dense matrix, rates and vectors in shared memory. The guard's
+// test runs in the call kernel's epilogue on the cell's result while it is still in shared memory, so a result is
+// written to HBM once; the recovery kernel recomputes only the cells the guard listed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "device.cuh"
+
+using namespace mx;
+
+namespace {
+
+constexpr int WARPS = 4;  // warps per cell
+
+// The call kernel: screening, rates, Rodas3 steps, output and the guard, per cell (call.cuh:5-177, guard.cuh:114-140).
+template <int W, int R>
+__global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallArgs a) {
+  extern __shared__ double smem[];
+  const Cell c = cell_arrays(net, smem);
+  const int tid = (int)threadIdx.x, nt = 32 * W, lane = tid & 31, warp = tid >> 5, ns = net.ns, ld = net.ld;
+  int cell = (int)blockIdx.x;
+  while (cell < a.B) {
+    const double Tc = a.T[cell], dt = a.dt[cell], hin = a.h_in[cell];
+    const double nd = a.P[cell] / (MX_KB * Tc);
+    const double* x0 = a.x + (size_t)cell * ns;
+    const double* Jc = a.J + (size_t)cell * net.nj;
+    for (int i = tid; i < ns; i += nt) c.N[i] = x0[__ldg(net.perm + i)];
+    __syncthreads();
+    if (warp == 0) {  // screening on one warp, in the warp's own summation order (common.cuh:246-279)
+      const double nan = __longlong_as_double(0x7ff8000000000000ll);
+      double p = 0.0, pm = 0.0;
+      for (int i = lane; i < ns; i += 32) {
+        const double xi = c.N[i];
+        p += xi >= 0.0 ? xi : nan;
+        pm = fmax(pm, xi);
+      }
+      for (int b = lane; b < net.nj; b += 32) {
+        const double q = Jc[b];
+        p += q >= 0.0 ? 0.0 * q : nan;
+      }
+      const double ps = warp_sum(p), mxv = warp_max(pm);
+      const bool forcing = isfinite(Tc) && isfinite(nd) && nd > 0.0 && isfinite(dt) && dt >= 0.0;
+      const bool fine = fabs(ps - 1.0) <= MX_X_SUM_TOL && mxv > 0.0 && forcing;
+      const int st = Tc < MX_T_MIN ? MX_REFUSED_COLD : (Tc > MX_T_MAX ? MX_REFUSED_HOT : (fine ? 0 : MX_REFUSED_BAD_INPUT));
+      if (lane == 0) {
+        c.ints[0] = st;
+        a.status[cell] = st;
+        if (!isfinite(hin)) atomicAdd(a.count + MX_COUNT_NONFINITE_H, 1);
+      }
+    }
+    __syncthreads();
+    const int st = c.ints[0];
+    if (st == 0) cell_rates(net, c, Tc, nd, Jc, tid, nt);
+    const double h0 = isfinite(hin) ? hin : dt;  // a non-finite h acts as dt
+    StepState s = {fmax(fmin(h0, dt), MX_H_MIN), 0.0, 0.0, 0.0, 0.0, false};
+    int it = (dt > 0.0 && st == 0) ? 0 : a.max_steps;  // a refused cell takes no step
+    double c0 = 0.0;
+    int tries = 0, retries = 0;
+    while (it < a.max_steps && s.t < dt * MX_CALL_END) {
+      const double ha = fmin(s.h, dt - s.t), igh = 1.0 / (GAMMA * ha), ih = 1.0 / ha;
+      tries++;
+      retries += s.prej ? 1 : 0;
+      // F, u and -Jn at N: a retry after a rejection recomputes those of the rejected try, bit for bit
+      const double ntot = rhs(net, c, c.N, true, nd, tid, nt);
+      jacobian_w(net, c, ntot, tid, nt);
+      for (int i = tid; i < ns; i += nt) c.A[i * ld + i] += igh;  // M0 = I / (gamma h) - Jn
+      __syncthreads();
+      lu_factor(net, c.A, c.dinv, tid, nt);
+      if (warp == 0) {  // stages 1 and 2: K1 and M0^-1 w together, then Sherman-Morrison
+        for (int i = lane; i < ns; i += 32) c.K1[i] = c.F[i];
+        __syncwarp();
+        lu_solve<R, 2>(net, c.A, c.dinv, c.K1, c.U, lane);
+        c0 = 1.0 / (1.0 - lane_sum(c.U, ns, lane));
+        sherman(net, c.K1, c.U, c0, lane);
+        for (int i = lane; i < ns; i += 32) c.K2[i] = fma(RODAS_C21 * ih, c.K1[i], c.F[i]);
+        __syncwarp();
+        lu_solve<R, 1>(net, c.A, c.dinv, c.K2, nullptr, lane);
+        sherman(net, c.K2, c.U, c0, lane);
+        for (int i = lane; i < ns; i += 32) c.Y[i] = c.N[i] + 2.0 * c.K1[i];
+      }
+      __syncthreads();
+      rhs(net, c, c.Y, false, nd, tid, nt);
+      if (warp == 0) {  // stage 3
+        for (int i = lane; i < ns; i += 32) c.K3[i] = fma(ih, c.K1[i] - c.K2[i], c.F[i]);
+        __syncwarp();
+        lu_solve<R, 1>(net, c.A, c.dinv, c.K3, nullptr, lane);
+        sherman(net, c.K3, c.U, c0, lane);
+        for (int i = lane; i < ns; i += 32) c.Y[i] = c.N[i] + 2.0 * c.K1[i] + c.K3[i];
+      }
+      __syncthreads();
+      rhs(net, c, c.Y, false, nd, tid, nt);
+      if (warp == 0) {  // stage 4 and the error
+        for (int i = lane; i < ns; i += 32)
+          c.K4[i] = fma(ih, fma(-RODAS_C43, c.K3[i], c.K1[i] - c.K2[i]), c.F[i]);
+        __syncwarp();
+        lu_solve<R, 1>(net, c.A, c.dinv, c.K4, nullptr, lane);
+        sherman(net, c.K4, c.U, c0, lane);
+        try_error(net, c, s.t == 0.0, a.rtol, a.atol, lane);
+      }
+      __syncthreads();
+      const double en = c.red[0];
+      const bool ok = c.red[1] != 0.0;
+      if (ok) {
+        for (int i = tid; i < ns; i += nt) c.N[i] = fmax(c.Y[i], 0.0);
+        s.t += ha;
+        s.nok += 1.0;
+      }
+      const double fac = step_factor(en, ok, s.prej, s.pen, s.pha, ha);
+      s.h = ha * fac;
+      s.prej = !ok;
+      s.pen = en;
+      s.pha = ha;
+      it++;
+      __syncthreads();
+    }
+    // x = N / sum N in the network's order (write_state), then the guard on it (check_cell)
+    if (warp == 0) {
+      const double sum = lane_sum(c.N, ns, lane);
+      if (lane == 0) c.red[3] = sum;
+    }
+    __syncthreads();
+    const double sum = c.red[3];
+    for (int i = tid; i < ns; i += nt) c.Y[__ldg(net.perm + i)] = c.N[i] / sum;
+    __syncthreads();
+    if (tid == 0) {
+      const int done = (st == 0 && s.t >= dt * MX_CALL_END) ? 1 : 0;
+      a.h_out[cell] = s.h;
+      a.done[cell] = done;
+      a.steps[cell] = s.nok;
+      int r = 0;
+      if (st == MX_REFUSED_COLD)
+        atomicAdd(a.count + MX_COUNT_COLD, 1);
+      else if (st == MX_REFUSED_HOT)
+        atomicAdd(a.count + MX_COUNT_HOT, 1);
+      else if (st == MX_REFUSED_BAD_INPUT)
+        atomicAdd(a.count + MX_COUNT_BAD_INPUT, 1);
+      else {
+        const int g = check_cell(net, x0, c.Y, done, s.nok, a.atol);
+        if (g & GUARD_NONFINITE) atomicAdd(a.count + MX_COUNT_NONFINITE, 1);
+        if (g & GUARD_UNFINISHED) atomicAdd(a.count + MX_COUNT_UNFINISHED, 1);
+        if (g & GUARD_DRIFT) atomicAdd(a.count + MX_COUNT_DRIFT, 1);
+        if (g) {
+          r = 1;
+          a.list[atomicAdd(a.count + MX_COUNT_RECOMPUTED, 1)] = cell;
+        }
+      }
+      a.flag[cell] = r;
+      if (a.tries) {
+        atomicAdd(a.tries, (unsigned long long)tries);
+        atomicAdd(a.tries + 1, (unsigned long long)retries);
+      }
+      c.ints[1] = (int)(gridDim.x + atomicAdd(a.count + MX_COUNT_QUEUE, 1));
+    }
+    __syncthreads();
+    double* xo = a.x_out + (size_t)cell * ns;
+    for (int i = tid; i < ns; i += nt) xo[i] = c.Y[i];
+    cell = c.ints[1];
+    __syncthreads();
+  }
+}
+
+// The recovery: listed cells recomputed from their inputs with the dense W = I / (gamma h) - Jn - w 1^T factored with
+// threshold pivoting, REC_STEPS times the tries, and up to REC_RETRIES retries with a smaller first try when only the
+// element test failed (recover.cuh:231-310).
+template <int W, int R>
+__global__ void __launch_bounds__(32 * W) recover_kernel(const Net net, const CallArgs a, int max_steps) {
+  const int nfl = a.count[MX_COUNT_RECOMPUTED];
+  if ((int)blockIdx.x >= nfl) return;
+  extern __shared__ double smem[];
+  const Cell c = cell_arrays(net, smem);
+  const int tid = (int)threadIdx.x, nt = 32 * W, lane = tid & 31, warp = tid >> 5, ns = net.ns, ld = net.ld;
+  int* pr = c.ints + 4;
+  int q = (int)blockIdx.x;
+  while (q < nfl) {
+    const int cell = a.list[q];
+    const double Tc = a.T[cell], dt = a.dt[cell], hin = a.h_in[cell];
+    const double nd = a.P[cell] / (MX_KB * Tc);
+    const double* x0 = a.x + (size_t)cell * ns;
+    const double* Jc = a.J + (size_t)cell * net.nj;
+    cell_rates(net, c, Tc, nd, Jc, tid, nt);  // a listed cell passed the screening (status 0)
+    const double h0 = isfinite(hin) ? hin : dt, m = fmin(h0, dt);
+    for (int k = 0;; k++) {
+      for (int i = tid; i < ns; i += nt) c.N[i] = x0[__ldg(net.perm + i)];
+      __syncthreads();
+      const double start = k == 0 ? m : fmin(m, dt * pow(MX_REC_RETRY_SPLIT, (double)k));
+      StepState s = {fmax(start, MX_H_MIN), 0.0, 0.0, 0.0, 0.0, false};
+      int it = dt > 0.0 ? 0 : max_steps;
+      while (it < max_steps && s.t < dt * MX_CALL_END) {
+        const double ha = fmin(s.h, dt - s.t), igh = 1.0 / (GAMMA * ha), ih = 1.0 / ha;
+        if (tid == 0 && a.tries) atomicAdd(a.tries + 2, 1ull);
+        const double ntot = rhs(net, c, c.N, true, nd, tid, nt);
+        jacobian_w(net, c, ntot, tid, nt);
+        for (int e = tid; e < ns * ns; e += nt) {  // form_dense_w
+          const int i = e / ns, j = e - i * ns;
+          double* p = c.A + i * ld + j;
+          *p = (i == j ? *p + igh : *p) - c.U[i];
+        }
+        __syncthreads();
+        if (warp == 0) {
+          for (int i = lane; i < ns; i += 32) c.K1[i] = c.F[i];
+          __syncwarp();
+          dense_lu_pivot(net, c.A, c.dinv, pr, lane);
+          dense_solve<R>(net, c.A, c.dinv, pr, c.K1, lane);
+          for (int i = lane; i < ns; i += 32) c.K2[i] = fma(RODAS_C21 * ih, c.K1[i], c.F[i]);
+          __syncwarp();
+          dense_solve<R>(net, c.A, c.dinv, pr, c.K2, lane);
+          for (int i = lane; i < ns; i += 32) c.Y[i] = c.N[i] + 2.0 * c.K1[i];
+        }
+        __syncthreads();
+        rhs(net, c, c.Y, false, nd, tid, nt);
+        if (warp == 0) {
+          for (int i = lane; i < ns; i += 32) c.K3[i] = fma(ih, c.K1[i] - c.K2[i], c.F[i]);
+          __syncwarp();
+          dense_solve<R>(net, c.A, c.dinv, pr, c.K3, lane);
+          for (int i = lane; i < ns; i += 32) c.Y[i] = c.N[i] + 2.0 * c.K1[i] + c.K3[i];
+        }
+        __syncthreads();
+        rhs(net, c, c.Y, false, nd, tid, nt);
+        if (warp == 0) {
+          for (int i = lane; i < ns; i += 32)
+            c.K4[i] = fma(ih, fma(-RODAS_C43, c.K3[i], c.K1[i] - c.K2[i]), c.F[i]);
+          __syncwarp();
+          dense_solve<R>(net, c.A, c.dinv, pr, c.K4, lane);
+          try_error(net, c, s.t == 0.0, a.rtol, a.atol, lane);
+        }
+        __syncthreads();
+        const double en = c.red[0];
+        const bool ok = c.red[1] != 0.0;
+        if (ok) {
+          for (int i = tid; i < ns; i += nt) c.N[i] = fmax(c.Y[i], 0.0);
+          s.t += ha;
+          s.nok += 1.0;
+        }
+        const double fac = step_factor(en, ok, s.prej, s.pen, s.pha, ha);
+        s.h = ha * fac;
+        s.prej = !ok;
+        s.pen = en;
+        s.pha = ha;
+        it++;
+        __syncthreads();
+      }
+      if (warp == 0) {
+        const double sum = lane_sum(c.N, ns, lane);
+        if (lane == 0) c.red[3] = sum;
+      }
+      __syncthreads();
+      const double sum = c.red[3];
+      for (int i = tid; i < ns; i += nt) c.Y[__ldg(net.perm + i)] = c.N[i] / sum;
+      __syncthreads();
+      if (tid == 0) {
+        const int dn = s.t >= dt * MX_CALL_END ? 1 : 0;
+        const int g = check_cell(net, x0, c.Y, dn, s.nok, a.atol);
+        if (g == GUARD_DRIFT && k < MX_REC_RETRIES) {
+          c.ints[1] = -1;  // only the element test failed: again from the inputs with a smaller first try
+        } else {
+          a.h_out[cell] = s.h;
+          a.done[cell] = g ? 0 : dn;
+          a.steps[cell] = s.nok;
+          a.flag[cell] = g ? 2 : 1;
+          atomicAdd(a.count + (g ? MX_COUNT_STILL_FAILED : MX_COUNT_RECOVERED), 1);
+          c.ints[1] = (int)(gridDim.x + atomicAdd(a.count + MX_COUNT_RECOVERY_QUEUE, 1));
+        }
+      }
+      __syncthreads();
+      double* xo = a.x_out + (size_t)cell * ns;
+      for (int i = tid; i < ns; i += nt) xo[i] = c.Y[i];
+      const int nq = c.ints[1];
+      __syncthreads();
+      if (nq >= 0) {
+        q = nq;
+        break;
+      }
+    }
+  }
+}
+
+// The guard alone, one thread per cell (guard.cuh:114-140), on results in global memory.
+__global__ void guard_kernel(const Net net, const double* x0, double* xout, const int* done, const double* nok,
+                             const int* status, int B, double atol, int* flag, int* count, int* list) {
+  const int cell = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (cell >= B) return;
+  const int s = status[cell];
+  int r = 0;
+  if (s == MX_REFUSED_COLD)
+    atomicAdd(count + MX_COUNT_COLD, 1);
+  else if (s == MX_REFUSED_HOT)
+    atomicAdd(count + MX_COUNT_HOT, 1);
+  else if (s == MX_REFUSED_BAD_INPUT)
+    atomicAdd(count + MX_COUNT_BAD_INPUT, 1);
+  else {
+    const int g = check_cell(net, x0 + (size_t)cell * net.ns, xout + (size_t)cell * net.ns, done[cell], nok[cell],
+                             atol);
+    if (g & GUARD_NONFINITE) atomicAdd(count + MX_COUNT_NONFINITE, 1);
+    if (g & GUARD_UNFINISHED) atomicAdd(count + MX_COUNT_UNFINISHED, 1);
+    if (g & GUARD_DRIFT) atomicAdd(count + MX_COUNT_DRIFT, 1);
+    if (g) {
+      r = 1;
+      list[atomicAdd(count + MX_COUNT_RECOMPUTED, 1)] = cell;
+    }
+  }
+  flag[cell] = r;
+}
+
+__global__ void add_counts_kernel(const int* count, long long* total) {
+  const int i = (int)threadIdx.x;
+  if (i < MX_COUNT_SLOTS) total[i] += count[i];
+}
+
+typedef void (*CallFn)(const Net, const CallArgs);
+typedef void (*RecoverFn)(const Net, const CallArgs, int);
+
+constexpr int RCLASSES[] = {1, 2, 3, 4, 8};  // rows per lane of the warp solves: species up to 32, 64, 96, 128, 256
+
+template <int R>
+void kernels_for(CallFn* call, RecoverFn* rec) {
+  *call = call_kernel<WARPS, R>;
+  *rec = recover_kernel<WARPS, R>;
+}
+
+bool pick_kernels(int ns, CallFn* call, RecoverFn* rec, int* r) {
+  const int need = (ns + 31) / 32;
+  if (need <= 1) { kernels_for<1>(call, rec); *r = 1; return true; }
+  if (need <= 2) { kernels_for<2>(call, rec); *r = 2; return true; }
+  if (need <= 3) { kernels_for<3>(call, rec); *r = 3; return true; }
+  if (need <= 4) { kernels_for<4>(call, rec); *r = 4; return true; }
+  if (need <= 8) { kernels_for<8>(call, rec); *r = 8; return true; }
+  return false;
+}
+
+void set_error(char* err, size_t len, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
+void set_error(char* err, size_t len, const char* fmt, ...) {
+  if (!err || !len) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(err, len, fmt, ap);
+  va_end(ap);
+}
+
+// Restores the caller's current device on scope exit.
+struct DeviceScope {
+  int old = -1;
+  cudaError_t status;
+  explicit DeviceScope(int dev) {
+    cudaGetDevice(&old);
+    status = cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    if (old >= 0) cudaSetDevice(old);
+  }
+};
+
+}  // namespace
+
+struct mx_solver {
+  int device = 0;
+  Net net{};
+  std::vector<void*> buffers;
+  CallFn call = nullptr;
+  RecoverFn recover = nullptr;
+  int rows_per_lane = 0;
+  size_t smem = 0;
+  int sms = 0, call_ctas = 0, recover_ctas = 0;
+  int* list = nullptr;
+  int64_t list_capacity = 0;
+  unsigned long long* tries = nullptr;
+};
+
+namespace {
+
+template <typename T>
+cudaError_t upload(mx_solver* s, const T* host, size_t count, const T** dev) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return e;
+  s->buffers.push_back(p);
+  if (count) e = cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice);
+  *dev = (const T*)p;
+  return e;
+}
+
+void release(mx_solver* s) {
+  for (void* p : s->buffers) cudaFree(p);
+  s->buffers.clear();
+  if (s->list) cudaFree(s->list);
+  s->list = nullptr;
+}
+
+}  // namespace
+
+extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solver** out, char* err, size_t errlen) {
+  if (!n || !out) {
+    set_error(err, errlen, "mx_create: null network or output");
+    return MX_ERR_ARGUMENT;
+  }
+  *out = nullptr;
+  if (n->ns < 1 || n->ns > MX_MAX_SPECIES || n->nr < 0 || n->nr >= 2048 || n->nel < 1 || n->nel > MX_MAX_ELEMENTS ||
+      n->nj != n->nr - n->nrt || n->n_entries < 0) {
+    set_error(err, errlen, "mx_create: network sizes out of range (ns %d, nr %d, nel %d)", n->ns, n->nr, n->nel);
+    return MX_ERR_NETWORK;
+  }
+  if (!(drift >= 0.0 && drift <= 1e300)) {
+    set_error(err, errlen, "drift: a finite allowance of at least 0 expected, got %g", drift);
+    return MX_ERR_ARGUMENT;
+  }
+  DeviceScope scope(device);
+  if (scope.status != cudaSuccess) {
+    set_error(err, errlen, "mx_create: device %d: %s", device, cudaGetErrorString(scope.status));
+    return MX_ERR_CUDA;
+  }
+  mx_solver* s = new (std::nothrow) mx_solver();
+  if (!s) return MX_ERR_CUDA;
+  s->device = device;
+  Net& net = s->net;
+  const int ns = n->ns, nr = n->nr;
+  net.ns = ns;
+  net.nr = nr;
+  net.nrt = n->nrt;
+  net.nj = n->nj;
+  net.nel = n->nel;
+  net.n_entries = n->n_entries;
+  net.drift = drift;
+  double etot = 0.0;
+  for (int i = 0; i < ns * n->nel; i++) etot += n->atoms[i];
+  net.etot = etot;
+  if (!pick_kernels(ns, &s->call, &s->recover, &s->rows_per_lane)) {
+    delete s;
+    return MX_ERR_NETWORK;
+  }
+  // shared-memory layout of one cell (doubles): A [ns][ld], kf kr, v (or G/RT), n, N Y F U K1-K4 dinv, red, ints
+  net.ld = ns | 1;  // odd: a column of A is read without bank conflicts
+  int off = 0;
+  auto take = [&](int doubles) {
+    const int o = off;
+    off += (doubles + 1) & ~1;
+    return o;
+  };
+  net.oA = take(ns * net.ld);
+  net.oK = take(2 * nr + 2);
+  net.oV = take(std::max(nr, ns + 1));
+  net.on = take(ns + 1);
+  net.oN = take(ns);
+  net.oY = take(ns);
+  net.oF = take(ns);
+  net.oU = take(ns);
+  net.oK1 = take(ns);
+  net.oK2 = take(ns);
+  net.oK3 = take(ns);
+  net.oK4 = take(ns);
+  net.oD = take(ns);
+  net.oRed = take(8);
+  net.oInts = take((ns + 8) / 2 + 1);
+  net.doubles = off;
+  s->smem = (size_t)off * sizeof(double);
+
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
+  if ((size_t)optin < s->smem) {
+    set_error(err, errlen, "one cell needs %zu B of shared memory; the device has %d per block", s->smem, optin);
+    delete s;
+    return MX_ERR_NETWORK;
+  }
+  cudaError_t e = cudaFuncSetAttribute((const void*)s->call, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)s->recover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->call_ctas, (const void*)s->call, 32 * WARPS, s->smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->recover_ctas, (const void*)s->recover, 32 * WARPS, s->smem);
+  if (e == cudaSuccess && (s->call_ctas < 1 || s->recover_ctas < 1)) e = cudaErrorInvalidConfiguration;
+  // the tables
+  std::vector<uint64_t> rx8(nr);
+  for (int r = 0; r < nr; r++) {
+    uint64_t w = 0;
+    for (int q = 0; q < 6; q++) w |= (uint64_t)n->rx[6 * r + q] << (8 * q);
+    rx8[r] = w;
+  }
+  const int nsv = n->sv_ptr[ns], njt = n->jac_ptr[n->n_entries];
+  if (e == cudaSuccess) e = upload(s, n->perm, ns, &net.perm);
+  if (e == cudaSuccess) e = upload(s, rx8.data(), nr, &net.rx8);
+  if (e == cudaSuccess) e = upload(s, n->rc, (size_t)nr * 14, &net.rc);
+  if (e == cudaSuccess) e = upload(s, n->rf, nr, &net.rf);
+  if (e == cudaSuccess) e = upload(s, n->nasa, (size_t)2 * ns * 9, &net.nasa);
+  if (e == cudaSuccess) e = upload(s, n->atoms, (size_t)ns * n->nel, &net.atoms);
+  if (e == cudaSuccess) e = upload(s, n->sv_ptr, ns + 1, &net.sv_ptr);
+  if (e == cudaSuccess) e = upload(s, n->sv_term, nsv, &net.sv_term);
+  if (e == cudaSuccess) e = upload(s, n->jac_ptr, n->n_entries + 1, &net.jac_ptr);
+  if (e == cudaSuccess) e = upload(s, n->jac_entry, n->n_entries, &net.jac_entry);
+  if (e == cudaSuccess) e = upload(s, n->jac_term, njt, &net.jac_term);
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_create: %s", cudaGetErrorString(e));
+    release(s);
+    delete s;
+    return MX_ERR_CUDA;
+  }
+  *out = s;
+  return MX_OK;
+}
+
+static int grow_list(mx_solver* s, int64_t B, char* err, size_t errlen) {
+  if (B <= s->list_capacity) return MX_OK;
+  if (s->list) cudaFree(s->list);
+  s->list = nullptr;
+  s->list_capacity = 0;
+  const cudaError_t e = cudaMalloc(&s->list, (size_t)B * sizeof(int));
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_call: the recompute list of %lld cells: %s", (long long)B, cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  s->list_capacity = B;
+  return MX_OK;
+}
+
+extern "C" int mx_call(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
+                       const double* h_in, const double* J, int64_t B, double rtol, double atol, int32_t max_steps,
+                       double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag, int32_t* status,
+                       int32_t* count, int64_t* total, void* stream, char* err, size_t errlen) {
+  if (!s) {
+    set_error(err, errlen, "this solver was closed; build a new one");
+    return MX_ERR_CLOSED;
+  }
+  if (B < 0 || B > 0x7fffffff) {
+    set_error(err, errlen, "mx_call: B out of range: %lld", (long long)B);
+    return MX_ERR_ARGUMENT;
+  }
+  if (!(rtol > 0.0 && rtol < 1e300 && atol > 0.0 && atol < 1e300)) {
+    set_error(err, errlen, "rtol and atol finite and positive expected, got %g, %g", rtol, atol);
+    return MX_ERR_ARGUMENT;
+  }
+  if (max_steps < 1 || (int64_t)MX_REC_STEPS * max_steps > 0x7fffffff) {
+    set_error(err, errlen, "max_steps from 1 to %d expected, got %d", 0x7fffffff / MX_REC_STEPS, max_steps);
+    return MX_ERR_ARGUMENT;
+  }
+  if (!count || !total || (B > 0 && (!x || !T || !P || !dt || !h_in || !x_out || !h_out || !done || !steps ||
+                                     !flag || !status || (s->net.nj > 0 && !J)))) {
+    set_error(err, errlen, "mx_call: a required array is null");
+    return MX_ERR_ARGUMENT;
+  }
+  DeviceScope scope(s->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = grow_list(s, std::max<int64_t>(B, 1), err, errlen);
+  if (rc) return rc;
+  cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
+  if (e == cudaSuccess && B > 0) {
+    CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status, count,
+               s->list, s->tries};
+    const int grid = (int)std::min<int64_t>(B, (int64_t)s->call_ctas * s->sms);
+    s->call<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a);
+    const int rgrid = (int)std::min<int64_t>(B, (int64_t)s->recover_ctas * s->sms);
+    s->recover<<<rgrid, 32 * WARPS, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    add_counts_kernel<<<1, 32, 0, st>>>(count, (long long*)total);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_call: %s", cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  return MX_OK;
+}
+
+extern "C" int mx_guard(mx_solver* s, const double* x, double* x_out, const int32_t* done, const double* steps,
+                        const int32_t* status, int64_t B, double atol, int32_t* flag, int32_t* count, void* stream,
+                        char* err, size_t errlen) {
+  if (!s) {
+    set_error(err, errlen, "this solver was closed; build a new one");
+    return MX_ERR_CLOSED;
+  }
+  if (B < 0 || B > 0x7fffffff || !count || (B > 0 && (!x || !x_out || !done || !steps || !status || !flag))) {
+    set_error(err, errlen, "mx_guard: bad arguments");
+    return MX_ERR_ARGUMENT;
+  }
+  DeviceScope scope(s->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = grow_list(s, std::max<int64_t>(B, 1), err, errlen);
+  if (rc) return rc;
+  cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
+  if (e == cudaSuccess && B > 0) {
+    guard_kernel<<<(int)((B + 127) / 128), 128, 0, st>>>(s->net, x, x_out, done, steps, status, (int)B, atol, flag,
+                                                          count, s->list);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_guard: %s", cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  return MX_OK;
+}
+
+extern "C" int mx_info(const mx_solver* s, int32_t* values, int32_t n) {
+  if (!s || !values) return MX_ERR_ARGUMENT;
+  const int32_t v[] = {WARPS, s->rows_per_lane, (int32_t)s->smem, s->call_ctas, s->recover_ctas, s->sms, s->net.ld};
+  for (int i = 0; i < n && i < (int)(sizeof v / sizeof v[0]); i++) values[i] = v[i];
+  return MX_OK;
+}
+
+extern "C" int mx_destroy(mx_solver* s) {
+  if (!s) return MX_OK;
+  {
+    DeviceScope scope(s->device);
+    release(s);
+  }
+  delete s;
+  return MX_OK;
+}
+
+extern "C" int mx_set_try_counter(mx_solver* s, int64_t* tries) {
+  if (!s) return MX_ERR_CLOSED;
+  s->tries = (unsigned long long*)tries;
+  return MX_OK;
+}
+
+namespace {
+// Independent fma chains, for the FP64 issue peak of the device (a measurement of the roofline's denominator).
+__global__ void probe_fp64_kernel(double* out, long long iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) x[q] = threadIdx.x * 1e-7 + q;
+  for (long long i = 0; i < iters; i++) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) x[q] = fma(x[q], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) s += x[q];
+  if (s == 12345.678) out[0] = s;  // keeps the chains alive
+}
+}  // namespace
+
+extern "C" int mx_probe_fp64(int device, int64_t iters, double* gflops) {
+  if (!gflops || iters < 1) return MX_ERR_ARGUMENT;
+  DeviceScope scope(device);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  double* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double)) != cudaSuccess) return MX_ERR_CUDA;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sms * 8, threads = 256;
+  probe_fp64_kernel<<<blocks, threads>>>(out, iters / 10 + 1, 0.999999, 1e-9);  // warm-up
+  cudaEventRecord(e0);
+  probe_fp64_kernel<<<blocks, threads>>>(out, iters, 0.999999, 1e-9);
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess || ms <= 0.0f) return MX_ERR_CUDA;
+  *gflops = 2.0 * 8.0 * (double)iters * blocks * threads / (ms * 1e-3) / 1e9;
+  return MX_OK;
+}
+
+extern "C" const char* mx_version(void) { return "maxichem_b200 0.1 sm_100a"; }

@@ -1,0 +1,132 @@
+"""TEST INFRASTRUCTURE ONLY: the CPU oracle of the per-call chemistry solve (oracle/mx_oracle.c) through ctypes.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this package: as the checker of the CUDA
+path, or as the timed CPU baseline. The product (maxichem_b200) never imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+
+from maxichem_b200.abi import COUNT_SLOTS, NetworkStruct
+from maxichem_b200.tables import Tables
+
+HERE = Path(__file__).resolve().parent
+SOURCE = HERE / "mx_oracle.c"
+LIBRARY = HERE / "_build" / "libmx_oracle.so"
+FLAGS = ["-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-std=c11", "-Wall"]
+
+_lib: ctypes.CDLL | None = None
+
+
+def build(force: bool = False) -> Path:
+    """Compile the oracle with gcc (no contraction of multiply-adds: every fma is explicit)."""
+    LIBRARY.parent.mkdir(exist_ok=True)
+    header = HERE.parent / "include" / "maxichem_b200.h"
+    stale = not LIBRARY.exists() or max(SOURCE.stat().st_mtime, header.stat().st_mtime) > LIBRARY.stat().st_mtime
+    if force or stale:
+        tmp = LIBRARY.with_suffix(".tmp.so")
+        subprocess.run(["gcc", *FLAGS, str(SOURCE), "-o", str(tmp), "-lm"], check=True)
+        tmp.replace(LIBRARY)
+    return LIBRARY
+
+
+def library() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        lib = ctypes.CDLL(str(LIBRARY))
+        P, I64, D, I32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int32
+        lib.mxo_call.restype = ctypes.c_int
+        lib.mxo_call.argtypes = [P, D, P, P, P, P, P, P, I64, D, D, I32, P, P, P, P, P, P, P, ctypes.c_int]
+        lib.mxo_rates.restype = None
+        lib.mxo_rates.argtypes = [P, D, D, P, P, P, P]
+        lib.mxo_rhs_jacobian.restype = D
+        lib.mxo_rhs_jacobian.argtypes = [P, P, P, D, P, P, P]
+        lib.mxo_check_cell.restype = ctypes.c_int
+        lib.mxo_check_cell.argtypes = [P, P, P, ctypes.c_int, D, D, D]
+        lib.mxo_dense_lu.restype = None
+        lib.mxo_dense_lu.argtypes = [ctypes.c_int, P, P, P]
+        lib.mxo_dense_solve.restype = None
+        lib.mxo_dense_solve.argtypes = [ctypes.c_int, P, P, P, P, P]
+        lib.mxo_screen.restype = ctypes.c_int
+        lib.mxo_screen.argtypes = [P, P, D, D, D, P, P]
+        lib.mxo_threads.restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _f64(a: Any) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Oracle:
+    """The oracle for one network's tables: ``call`` mirrors CudaSolver.launch on host arrays."""
+
+    def __init__(self, tab: Tables, drift: float = 1e-6) -> None:
+        self.tab = tab
+        self.net = NetworkStruct(tab)
+        self.drift = float(drift)
+        self.lib = library()
+
+    def call(self, x: Any, T: Any, P: Any, dt: Any, h: Any, *, rtol: float = 1e-3, atol: float = 1e-25,
+             max_steps: int = 4000, J: Any = None, threads: int = 0) -> dict[str, np.ndarray]:
+        """One call on the CPU: x, h, done (bool), steps, flag, status and the counts (int32 [12])."""
+        x, T, P, dt, h = (_f64(a) for a in (x, T, P, dt, h))
+        B, ns = x.shape
+        Jc = _f64(J if J is not None and self.tab.nj else np.zeros((B, self.tab.nj)))
+        xo, ho, steps = np.empty_like(x), np.empty(B), np.empty(B)
+        done, flag, status = (np.empty(B, np.int32) for _ in range(3))
+        count = np.zeros(COUNT_SLOTS, np.int32)
+        self.lib.mxo_call(self.net.ref(), self.drift, _p(x), _p(T), _p(P), _p(dt), _p(h), _p(Jc), B, rtol, atol,
+                          max_steps, _p(xo), _p(ho), _p(done), _p(steps), _p(flag), _p(status), _p(count), threads)
+        return {"x": xo, "h": ho, "done": done.astype(bool), "steps": steps, "flag": flag, "status": status,
+                "count": count}  # fmt: skip
+
+    def rates(self, T: float, P: float, J: Any = None) -> tuple[np.ndarray, np.ndarray]:
+        tab = self.tab
+        kf, kr = np.empty(tab.nr), np.empty(tab.nr)
+        g = np.empty(tab.ns + 1)
+        Jc = _f64(J if J is not None else np.zeros(tab.nj))
+        nd = P / (1.380649e-16 * T)
+        self.lib.mxo_rates(self.net.ref(), T, nd, _p(Jc), _p(kf), _p(kr), _p(g))
+        return kf, kr
+
+    def rhs_jacobian(self, kf: np.ndarray, kr: np.ndarray, Y: np.ndarray, nd: float) -> tuple[Any, ...]:
+        """F, u0, -Jn (dense, elimination order) and n_tot at the state Y (elimination order)."""
+        ns = self.tab.ns
+        k = _f64(np.concatenate([kf, kr]))
+        Y = _f64(Y)
+        F, u0, A = np.empty(ns), np.empty(ns), np.empty((ns, ns))
+        ntot = self.lib.mxo_rhs_jacobian(self.net.ref(), _p(k), _p(Y), nd, _p(F), _p(u0), _p(A))
+        return F, u0, A, ntot
+
+
+def dense_lu(a: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """The recovery's threshold-pivoted dense LU: factors, 1 / pivots, row order."""
+    a = _f64(a).copy()
+    n = a.shape[0]
+    dinv, pr = np.empty(n), np.empty(n, np.int32)
+    library().mxo_dense_lu(n, _p(a), _p(dinv), _p(pr))
+    return a, dinv, pr
+
+
+def dense_solve(a: np.ndarray, dinv: np.ndarray, pr: np.ndarray, y: np.ndarray) -> np.ndarray:
+    y = _f64(y).copy()
+    work = np.empty_like(y)
+    library().mxo_dense_solve(len(y), _p(_f64(a)), _p(_f64(dinv)), _p(np.ascontiguousarray(pr, np.int32)), _p(y),
+                              _p(work))
+    return y
+
+
+def threads() -> int:
+    return int(library().mxo_threads())

@@ -1,0 +1,69 @@
+"""The parity rule between the CUDA path and the CPU oracle, shared by the GPU tests.
+
+Both sides run the same method on the same inputs; they differ only in the last bits of exp/log/pow (libm against
+CUDA's), so a cell either takes the same accepted steps on both sides, and then agrees to a relative RTOL per species
+above FLOOR, or (rarely) a rounding difference flips one accept/reject decision, and then the two results are two
+valid Rodas3 answers within the integrator's tolerance. The flips are counted and bounded.
+"""
+
+import numpy as np
+
+RTOL = 1e-9  # relative, per species above FLOOR, on cells whose accepted steps match (the north star's bar)
+FLOOR = 1e-20  # mole fraction
+FLIP_SHARE = 2e-3  # share of cells whose accepted steps may differ (a rounding-flipped accept/reject)
+FLIP_DEX = 0.1  # their worst difference above FLOOR, dex (the call's rtol 1e-3 on quantities far above atol)
+SHARE_TOL = 1e-11  # element shares of a passing cell, relative to the input's
+
+
+def shares(x: np.ndarray, atoms: np.ndarray) -> np.ndarray:
+    e = x @ atoms
+    return e / e.sum(1, keepdims=True)
+
+
+def compare(gpu: dict, ref: dict, x0: np.ndarray, atoms: np.ndarray) -> dict:
+    """Return the parity report of one call: GPU arrays (host numpy) against the oracle's."""
+    rep = {}
+    rep["status_equal"] = bool(np.array_equal(gpu["status"], ref["status"]))
+    rep["done_equal"] = bool(np.array_equal(gpu["done"], ref["done"]))
+    rep["flag_equal"] = bool(np.array_equal(gpu["flag"], ref["flag"]))
+    rep["counts_gpu"] = [int(v) for v in gpu["count"][1:-1]]
+    rep["counts_ref"] = [int(v) for v in ref["count"][1:-1]]
+    stepped = gpu["status"] == 0
+    same = (gpu["steps"] == ref["steps"]) & stepped
+    flips = stepped & ~same
+    rep["cells"] = int(len(gpu["steps"]))
+    rep["flips"] = int(flips.sum())
+    a, b = gpu["x"][same], ref["x"][same]
+    big = (np.abs(a) > FLOOR) & (np.abs(b) > FLOOR)
+    rel = np.abs(a - b) / np.maximum(np.abs(a), np.abs(b)).clip(1e-300)
+    rep["worst_rel"] = float(rel[big].max()) if big.any() else 0.0
+    hr = np.abs(gpu["h"][same] - ref["h"][same]) / np.abs(ref["h"][same]).clip(1e-300)
+    rep["worst_h_rel"] = float(hr.max()) if hr.size else 0.0
+    if flips.any():
+        la = np.log10(np.maximum(gpu["x"][flips], FLOOR))
+        lb = np.log10(np.maximum(ref["x"][flips], FLOOR))
+        rep["flip_dex"] = float(np.abs(la - lb).max())
+    else:
+        rep["flip_dex"] = 0.0
+    ok = (gpu["flag"] == 0) & stepped & np.isfinite(gpu["x"]).all(1)
+    if ok.any():
+        s0, s1 = shares(x0[ok], atoms), shares(gpu["x"][ok], atoms)
+        m = s0 > 1e-14
+        rep["share_rel"] = float((np.abs(s1 - s0)[m] / s0[m]).max())
+    else:
+        rep["share_rel"] = 0.0
+    return rep
+
+
+def passed(rep: dict, counts_exact: bool = True) -> bool:
+    return (
+        rep["status_equal"]
+        and (rep["done_equal"] or rep["flips"] > 0)
+        and (rep["flag_equal"] or rep["flips"] > 0)
+        and (not counts_exact or rep["counts_gpu"] == rep["counts_ref"] or rep["flips"] > 0)
+        and rep["worst_rel"] <= RTOL
+        and rep["worst_h_rel"] <= RTOL
+        and rep["flips"] <= max(1, FLIP_SHARE * rep["cells"])
+        and rep["flip_dex"] <= FLIP_DEX
+        and rep["share_rel"] <= SHARE_TOL
+    )
