@@ -130,6 +130,13 @@ int mx_guard(mx_solver* s, const double* x, double* x_out, const int32_t* done, 
 /* Launch layout of the solver (cells per CTA, warps per cell, CTAs per SM, shared bytes), for reports. */
 int mx_info(const mx_solver* s, int32_t* values, int32_t n);
 
+/* One fresh try of one cell (device x [ns], J [nj]) at try size h, with every stage written to the device array out:
+ * kf, kr [nr each], F, u0 [ns each], -Jn [ns][ns], w [ns], LU factors [ns][ns], dinv, K1, K2, K3, K4, N' [ns each],
+ * err, ok (elimination order). No counterpart in the reference: a test hook that runs the call kernel's own device
+ * functions, so each stage can be checked against the CPU oracle. */
+int mx_debug_try(mx_solver* s, const double* x, double T, double P, double h, const double* J, double rtol,
+                 double atol, double* out, void* stream);
+
 /* Register a device int64[3] that later calls of this solver add their tries to: [0] the call kernel's tries, [1] those
  * that followed a rejection, [2] the recovery's tries (NULL stops counting). No counterpart in the reference: it
  * feeds the measured roofline (algorithmic FLOPs per try are a property of the network's tables). */

@@ -86,6 +86,10 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "mx_info": (ctypes.c_int, [_P, _P, ctypes.c_int32]),
     "mx_destroy": (ctypes.c_int, [_P]),
     "mx_set_try_counter": (ctypes.c_int, [_P, _P]),
+    "mx_debug_try": (
+        ctypes.c_int,
+        [_P, _P, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, ctypes.c_double, ctypes.c_double, _P, _P],
+    ),
     "mx_probe_fp64": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
     "mx_version": (ctypes.c_char_p, []),
 }

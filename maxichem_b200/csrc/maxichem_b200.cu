@@ -284,6 +284,94 @@ __global__ void __launch_bounds__(32 * W) recover_kernel(const Net net, const Ca
   }
 }
 
+// One fresh try of one cell with every stage written out (a test hook that runs the call kernel's device functions):
+// out = kf, kr [nr each], F, u0 [ns each], -Jn [ns][ns], w [ns], LU factors [ns][ns], dinv, K1, K2, K3, K4, Y [ns each],
+// err, ok.
+template <int W, int R>
+__global__ void __launch_bounds__(32 * W) debug_try_kernel(const Net net, const double* x0, double Tc, double P,
+                                                           double ha, const double* Jc, double rtol, double atol,
+                                                           double* out) {
+  extern __shared__ double smem[];
+  const Cell c = cell_arrays(net, smem);
+  const int tid = (int)threadIdx.x, nt = 32 * W, lane = tid & 31, warp = tid >> 5, ns = net.ns, ld = net.ld;
+  const double nd = P / (MX_KB * Tc);
+  double* o = out;
+  for (int i = tid; i < ns; i += nt) c.N[i] = x0[__ldg(net.perm + i)];
+  __syncthreads();
+  cell_rates(net, c, Tc, nd, Jc, tid, nt);
+  for (int r = tid; r < net.nr; r += nt) {
+    o[r] = c.kf[r];
+    o[net.nr + r] = c.kr[r];
+  }
+  o += 2 * net.nr;
+  const double igh = 1.0 / (GAMMA * ha), ih = 1.0 / ha;
+  const double ntot = rhs(net, c, c.N, true, nd, tid, nt);
+  for (int i = tid; i < ns; i += nt) {
+    o[i] = c.F[i];
+    o[ns + i] = c.U[i];
+  }
+  o += 2 * ns;
+  __syncthreads();
+  jacobian_w(net, c, ntot, tid, nt);
+  // -Jn is in A before the diagonal; w in U
+  for (int e = tid; e < ns * ns; e += nt) o[e] = c.A[(e / ns) * ld + e % ns];
+  o += ns * ns;
+  for (int i = tid; i < ns; i += nt) o[i] = c.U[i];
+  o += ns;
+  __syncthreads();
+  for (int i = tid; i < ns; i += nt) c.A[i * ld + i] += igh;
+  __syncthreads();
+  lu_factor(net, c.A, c.dinv, tid, nt);
+  for (int e = tid; e < ns * ns; e += nt) o[e] = c.A[(e / ns) * ld + e % ns];
+  o += ns * ns;
+  for (int i = tid; i < ns; i += nt) o[i] = c.dinv[i];
+  o += ns;
+  double c0 = 0.0;
+  if (warp == 0) {
+    for (int i = lane; i < ns; i += 32) c.K1[i] = c.F[i];
+    __syncwarp();
+    lu_solve<R, 2>(net, c.A, c.dinv, c.K1, c.U, lane);
+    c0 = 1.0 / (1.0 - lane_sum(c.U, ns, lane));
+    sherman(net, c.K1, c.U, c0, lane);
+    for (int i = lane; i < ns; i += 32) c.K2[i] = fma(RODAS_C21 * ih, c.K1[i], c.F[i]);
+    __syncwarp();
+    lu_solve<R, 1>(net, c.A, c.dinv, c.K2, nullptr, lane);
+    sherman(net, c.K2, c.U, c0, lane);
+    for (int i = lane; i < ns; i += 32) c.Y[i] = c.N[i] + 2.0 * c.K1[i];
+  }
+  __syncthreads();
+  rhs(net, c, c.Y, false, nd, tid, nt);
+  if (warp == 0) {
+    for (int i = lane; i < ns; i += 32) c.K3[i] = fma(ih, c.K1[i] - c.K2[i], c.F[i]);
+    __syncwarp();
+    lu_solve<R, 1>(net, c.A, c.dinv, c.K3, nullptr, lane);
+    sherman(net, c.K3, c.U, c0, lane);
+    for (int i = lane; i < ns; i += 32) c.Y[i] = c.N[i] + 2.0 * c.K1[i] + c.K3[i];
+  }
+  __syncthreads();
+  rhs(net, c, c.Y, false, nd, tid, nt);
+  if (warp == 0) {
+    for (int i = lane; i < ns; i += 32) c.K4[i] = fma(ih, fma(-RODAS_C43, c.K3[i], c.K1[i] - c.K2[i]), c.F[i]);
+    __syncwarp();
+    lu_solve<R, 1>(net, c.A, c.dinv, c.K4, nullptr, lane);
+    sherman(net, c.K4, c.U, c0, lane);
+    try_error(net, c, true, rtol, atol, lane);
+  }
+  __syncthreads();
+  for (int i = tid; i < ns; i += nt) {
+    o[i] = c.K1[i];
+    o[ns + i] = c.K2[i];
+    o[2 * ns + i] = c.K3[i];
+    o[3 * ns + i] = c.K4[i];
+    o[4 * ns + i] = c.Y[i];
+  }
+  o += 5 * ns;
+  if (tid == 0) {
+    o[0] = c.red[0];
+    o[1] = c.red[1];
+  }
+}
+
 // The guard alone, one thread per cell (guard.cuh:114-140), on results in global memory.
 __global__ void guard_kernel(const Net net, const double* x0, double* xout, const int* done, const double* nok,
                              const int* status, int B, double atol, int* flag, int* count, int* list) {
@@ -317,23 +405,25 @@ __global__ void add_counts_kernel(const int* count, long long* total) {
 }
 
 typedef void (*CallFn)(const Net, const CallArgs);
+typedef void (*DebugFn)(const Net, const double*, double, double, double, const double*, double, double, double*);
 typedef void (*RecoverFn)(const Net, const CallArgs, int);
 
-constexpr int RCLASSES[] = {1, 2, 3, 4, 8};  // rows per lane of the warp solves: species up to 32, 64, 96, 128, 256
 
 template <int R>
-void kernels_for(CallFn* call, RecoverFn* rec) {
+void kernels_for(CallFn* call, RecoverFn* rec, DebugFn* dbg) {
   *call = call_kernel<WARPS, R>;
   *rec = recover_kernel<WARPS, R>;
+  *dbg = debug_try_kernel<WARPS, R>;
 }
 
-bool pick_kernels(int ns, CallFn* call, RecoverFn* rec, int* r) {
+// rows per lane of the warp solves: species up to 32, 64, 96, 128, 256
+bool pick_kernels(int ns, CallFn* call, RecoverFn* rec, DebugFn* dbg, int* r) {
   const int need = (ns + 31) / 32;
-  if (need <= 1) { kernels_for<1>(call, rec); *r = 1; return true; }
-  if (need <= 2) { kernels_for<2>(call, rec); *r = 2; return true; }
-  if (need <= 3) { kernels_for<3>(call, rec); *r = 3; return true; }
-  if (need <= 4) { kernels_for<4>(call, rec); *r = 4; return true; }
-  if (need <= 8) { kernels_for<8>(call, rec); *r = 8; return true; }
+  if (need <= 1) { kernels_for<1>(call, rec, dbg); *r = 1; return true; }
+  if (need <= 2) { kernels_for<2>(call, rec, dbg); *r = 2; return true; }
+  if (need <= 3) { kernels_for<3>(call, rec, dbg); *r = 3; return true; }
+  if (need <= 4) { kernels_for<4>(call, rec, dbg); *r = 4; return true; }
+  if (need <= 8) { kernels_for<8>(call, rec, dbg); *r = 8; return true; }
   return false;
 }
 
@@ -367,6 +457,7 @@ struct mx_solver {
   std::vector<void*> buffers;
   CallFn call = nullptr;
   RecoverFn recover = nullptr;
+  DebugFn debug = nullptr;
   int rows_per_lane = 0;
   size_t smem = 0;
   int sms = 0, call_ctas = 0, recover_ctas = 0;
@@ -433,7 +524,7 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   double etot = 0.0;
   for (int i = 0; i < ns * n->nel; i++) etot += n->atoms[i];
   net.etot = etot;
-  if (!pick_kernels(ns, &s->call, &s->recover, &s->rows_per_lane)) {
+  if (!pick_kernels(ns, &s->call, &s->recover, &s->debug, &s->rows_per_lane)) {
     delete s;
     return MX_ERR_NETWORK;
   }
@@ -474,6 +565,8 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   cudaError_t e = cudaFuncSetAttribute((const void*)s->call, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)s->recover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)s->debug, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->call_ctas, (const void*)s->call, 32 * WARPS, s->smem);
   if (e == cudaSuccess)
@@ -615,6 +708,14 @@ extern "C" int mx_destroy(mx_solver* s) {
   }
   delete s;
   return MX_OK;
+}
+
+extern "C" int mx_debug_try(mx_solver* s, const double* x, double T, double P, double h, const double* J, double rtol,
+                            double atol, double* out, void* stream) {
+  if (!s || !x || !out || (s->net.nj > 0 && !J)) return MX_ERR_ARGUMENT;
+  DeviceScope scope(s->device);
+  s->debug<<<1, 32 * WARPS, s->smem, (cudaStream_t)stream>>>(s->net, x, T, P, h, J, rtol, atol, out);
+  return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
 extern "C" int mx_set_try_counter(mx_solver* s, int64_t* tries) {

@@ -57,6 +57,8 @@ def library() -> ctypes.CDLL:
         lib.mxo_screen.restype = ctypes.c_int
         lib.mxo_screen.argtypes = [P, P, D, D, D, P, P]
         lib.mxo_threads.restype = ctypes.c_int
+        lib.mxo_debug_try.restype = None
+        lib.mxo_debug_try.argtypes = [P, P, D, D, D, P, D, D, P]
         _lib = lib
     return _lib
 
@@ -91,6 +93,15 @@ class Oracle:
                           max_steps, _p(xo), _p(ho), _p(done), _p(steps), _p(flag), _p(status), _p(count), threads)
         return {"x": xo, "h": ho, "done": done.astype(bool), "steps": steps, "flag": flag, "status": status,
                 "count": count}  # fmt: skip
+
+    def debug_try(self, x: Any, T: float, P: float, h: float, J: Any = None, rtol: float = 1e-3,
+                  atol: float = 1e-25) -> dict[str, np.ndarray]:
+        """One fresh try of one cell with every stage (the layout of the library's mx_debug_try)."""
+        tab = self.tab
+        out = np.empty(debug_size(tab))
+        Jc = _f64(J if J is not None and tab.nj else np.zeros(tab.nj))
+        self.lib.mxo_debug_try(self.net.ref(), _p(_f64(x)), T, P, h, _p(Jc), rtol, atol, _p(out))
+        return split_debug(tab, out)
 
     def rates(self, T: float, P: float, J: Any = None) -> tuple[np.ndarray, np.ndarray]:
         tab = self.tab
@@ -130,3 +141,19 @@ def dense_solve(a: np.ndarray, dinv: np.ndarray, pr: np.ndarray, y: np.ndarray) 
 
 def threads() -> int:
     return int(library().mxo_threads())
+
+
+def debug_size(tab: Tables) -> int:
+    return 2 * tab.nr + 10 * tab.ns + 2 * tab.ns * tab.ns + 2
+
+
+def split_debug(tab: Tables, out: np.ndarray) -> dict[str, np.ndarray]:
+    """Name the stages of a one-try dump."""
+    ns, nr = tab.ns, tab.nr
+    parts = [("kf", nr), ("kr", nr), ("F", ns), ("u0", ns), ("Jn", ns * ns), ("w", ns), ("LU", ns * ns), ("dinv", ns),
+             ("K1", ns), ("K2", ns), ("K3", ns), ("K4", ns), ("Y", ns), ("err", 1), ("ok", 1)]  # fmt: skip
+    d, o = {}, 0
+    for name, n in parts:
+        d[name] = out[o : o + n]
+        o += n
+    return d

@@ -652,6 +652,67 @@ double mxo_rhs_jacobian(const mx_network* net, const double* kf_kr, const double
   return ntot;
 }
 
+/* One fresh try of one cell with every stage written out, in the layout of the library's mx_debug_try. */
+void mxo_debug_try(const mx_network* net, const double* x0, double Tc, double P, double ha, const double* Jc,
+                   double rtol, double atol, double* out) {
+  const int ns = net->ns, nr = net->nr;
+  workspace w;
+  ws_alloc(&w, ns, nr);
+  cellctx c = {net, ns, nr, w.k, w.n, w.v};
+  const double nd = P / (MX_KB * Tc);
+  for (int i = 0; i < ns; i++) w.N[i] = x0[net->perm[i]];
+  mxo_rates(net, Tc, nd, Jc, w.k, w.k + nr, w.g);
+  double* o = out;
+  memcpy(o, w.k, sizeof(double) * 2 * nr);
+  o += 2 * nr;
+  const double igh = 1.0 / (GAMMA * ha), ih = 1.0 / ha;
+  const double ntot = rhs(&c, w.N, w.F, w.u, nd);
+  memcpy(o, w.F, sizeof(double) * ns);
+  memcpy(o + ns, w.u, sizeof(double) * ns);
+  o += 2 * ns;
+  jacobian(&c, w.A);
+  memcpy(o, w.A, sizeof(double) * ns * ns);
+  o += ns * ns;
+  add_w(ns, w.A, w.N, ntot, w.u);
+  memcpy(o, w.u, sizeof(double) * ns);
+  o += ns;
+  for (int i = 0; i < ns; i++) w.A[i * ns + i] += igh;
+  lu_factor(ns, w.A, w.dinv);
+  memcpy(o, w.A, sizeof(double) * ns * ns);
+  o += ns * ns;
+  memcpy(o, w.dinv, sizeof(double) * ns);
+  o += ns;
+  for (int i = 0; i < ns; i++) w.K1[i] = w.F[i];
+  lu_solve(ns, w.A, w.dinv, w.K1);
+  lu_solve(ns, w.A, w.dinv, w.u);
+  const double c0 = 1.0 / (1.0 - lane_sum(w.u, ns));
+  sherman(ns, w.K1, w.u, c0);
+  for (int i = 0; i < ns; i++) w.K2[i] = fma(C21 * ih, w.K1[i], w.F[i]);
+  lu_solve(ns, w.A, w.dinv, w.K2);
+  sherman(ns, w.K2, w.u, c0);
+  for (int i = 0; i < ns; i++) w.Y[i] = w.N[i] + 2.0 * w.K1[i];
+  rhs(&c, w.Y, w.F, NULL, nd);
+  for (int i = 0; i < ns; i++) w.K3[i] = fma(ih, w.K1[i] - w.K2[i], w.F[i]);
+  lu_solve(ns, w.A, w.dinv, w.K3);
+  sherman(ns, w.K3, w.u, c0);
+  for (int i = 0; i < ns; i++) w.Y[i] = w.N[i] + 2.0 * w.K1[i] + w.K3[i];
+  rhs(&c, w.Y, w.F, NULL, nd);
+  for (int i = 0; i < ns; i++) w.K4[i] = fma(ih, fma(-C43, w.K3[i], w.K1[i] - w.K2[i]), w.F[i]);
+  lu_solve(ns, w.A, w.dinv, w.K4);
+  sherman(ns, w.K4, w.u, c0);
+  int ok = 0;
+  const double en = try_error(ns, w.N, w.K1, w.K3, w.K4, w.Y, 1, rtol, atol, &ok);
+  memcpy(o, w.K1, sizeof(double) * ns);
+  memcpy(o + ns, w.K2, sizeof(double) * ns);
+  memcpy(o + 2 * ns, w.K3, sizeof(double) * ns);
+  memcpy(o + 3 * ns, w.K4, sizeof(double) * ns);
+  memcpy(o + 4 * ns, w.Y, sizeof(double) * ns);
+  o += 5 * ns;
+  o[0] = en;
+  o[1] = ok;
+  ws_free(&w);
+}
+
 int mxo_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

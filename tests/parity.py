@@ -37,6 +37,13 @@ def compare(gpu: dict, ref: dict, x0: np.ndarray, atoms: np.ndarray) -> dict:
     big = (np.abs(a) > FLOOR) & (np.abs(b) > FLOOR)
     rel = np.abs(a - b) / np.maximum(np.abs(a), np.abs(b)).clip(1e-300)
     rep["worst_rel"] = float(rel[big].max()) if big.any() else 0.0
+    per_cell = np.where(big, rel, 0.0).max(1)
+    idx = np.flatnonzero(same)[np.argsort(per_cell)[::-1][:4]]
+    rep["worst_cells"] = [
+        (int(c), float(np.where(big, rel, 0.0).max(1)[list(np.flatnonzero(same)).index(c)]), float(gpu["steps"][c]),
+         int(gpu["flag"][c]), int(ref["flag"][c]), float(gpu["h"][c]), float(ref["h"][c]))
+        for c in idx
+    ]
     hr = np.abs(gpu["h"][same] - ref["h"][same]) / np.abs(ref["h"][same]).clip(1e-300)
     rep["worst_h_rel"] = float(hr.max()) if hr.size else 0.0
     if flips.any():
