@@ -12,9 +12,10 @@ pytestmark = pytest.mark.gpu
 
 
 def _rel(a, b):
-    scale = np.maximum(np.abs(a), np.abs(b))
-    m = scale > 1e-300
-    return float((np.abs(a - b)[m] / scale[m]).max()) if m.any() else 0.0
+    """Largest difference relative to the vector's largest entry (a component far below it carries the rounding of
+    its larger neighbours, so it is not judged against itself)."""
+    scale = max(np.abs(a).max(), np.abs(b).max())
+    return float(np.abs(a - b).max() / scale) if scale > 0 else 0.0
 
 
 @pytest.mark.parametrize("name", ["cho41", "chno69"])
@@ -38,7 +39,7 @@ def test_each_stage_of_one_try_matches_the_oracle(gpu, networks, name):
             for k in g:
                 worst[k] = max(worst.get(k, 0.0), _rel(g[k], r[k]))
         print(name, {k: f"{v:.1e}" for k, v in worst.items()})
-        for k in ("kf", "kr"):
+        for k in ("kf", "kr", "F", "u0", "Jn", "dinv", "Y", "err"):
             assert worst[k] < 1e-13, (k, worst[k])
-        for k in ("F", "u0", "Jn", "w", "LU", "dinv"):
-            assert worst[k] < 1e-9, (k, worst[k])
+        for k in ("w", "LU", "K1", "K2", "K3", "K4"):
+            assert worst[k] < 1e-10, (k, worst[k])
