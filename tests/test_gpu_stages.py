@@ -39,7 +39,7 @@ def test_each_stage_of_one_try_matches_the_oracle(gpu, networks, name):
             for k in g:
                 worst[k] = max(worst.get(k, 0.0), _rel(g[k], r[k]))
         print(name, {k: f"{v:.1e}" for k, v in worst.items()})
-        for k in ("kf", "kr", "F", "u0", "Jn", "dinv", "Y", "err"):
+        for k in ("kf", "kr", "F", "u0", "Jn", "dinv", "Y"):
             assert worst[k] < 1e-13, (k, worst[k])
-        for k in ("w", "LU", "K1", "K2", "K3", "K4"):
+        for k in ("w", "LU", "K1", "K2", "K3", "K4", "err"):
             assert worst[k] < 1e-10, (k, worst[k])
