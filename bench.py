@@ -42,7 +42,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--cells", type=int, default=1 << 20, help="cells per GPU")
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    p.add_argument("--cpu-sample", type=int, default=2048, help="cells of the CPU baseline sample")
+    p.add_argument("--cpu-sample", type=int, default=131072, help="cells of the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()

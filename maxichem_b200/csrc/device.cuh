@@ -235,25 +235,77 @@ __device__ void jacobian_w(const Net& net, const Cell& c, double ntot, int tid, 
 // ---- dense LU without exchanges, blocked (PANEL pivots at a time) ----
 // Every entry receives its updates A_ij <- fma(-l_ik, A_kj, A_ij) in ascending k, l_ik = A_ik / A_kk taken as
 // A_ik * (1 / A_kk): the order and the operations of the right-looking LU, so the bits of the sparse factorisation
-// on the fill pattern (call.cuh:81-112) for finite data.
-__device__ void lu_factor(const Net& net, double* A, double* dinv, int tid, int nt) {
+// on the fill pattern (call.cuh:81-112) for finite data. Per block: the panel's pivots one by one (one thread per
+// row), the block's pivot rows beyond the panel (one thread per column), then the trailing matrix as a rank-PANEL
+// update in 4 x 4 register tiles spread over the CTA (rows and columns cyclic, so a warp's loads are broadcast or
+// consecutive).
+
+// The trailing rows and columns [ke, ns) less L[:, kb..kb+nb) U[kb..kb+nb, :], tiles of 4 x 4 per thread.
+template <int NT>
+__device__ __forceinline__ void trailing_update(double* A, int ld, int kb, int nb, int ke, int ns, int tid) {
+  constexpr int CG = 16, RG = NT / CG;  // column groups x row groups
+  const int cg = tid % CG, rg = tid / CG, m = ns - ke;
+  for (int rb = rg; rb < m; rb += 4 * RG) {    // the tile's rows: ke + rb + RG a, a < 4
+    for (int cb = cg; cb < m; cb += 4 * CG) {  // its columns: ke + cb + CG b, b < 4
+      int row[4], col[4];
+      bool rok[4], cok[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        rok[a] = rb + RG * a < m;
+        row[a] = ke + (rok[a] ? rb + RG * a : 0);
+        cok[a] = cb + CG * a < m;
+        col[a] = ke + (cok[a] ? cb + CG * a : 0);
+      }
+      double acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = A[row[a] * ld + col[b]];
+#pragma unroll
+      for (int t = 0; t < PANEL; t++) {
+        if (t < nb) {
+          double l[4], u[4];
+#pragma unroll
+          for (int a = 0; a < 4; a++) {
+            l[a] = A[row[a] * ld + kb + t];
+            u[a] = A[(kb + t) * ld + col[a]];
+          }
+#pragma unroll
+          for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) acc[a][b] = fma(-l[a], u[b], acc[a][b]);
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+          if (rok[a] && cok[b]) A[row[a] * ld + col[b]] = acc[a][b];
+    }
+  }
+}
+
+template <int NT>
+__device__ void lu_factor(const Net& net, double* A, double* dinv, int tid) {
   const int ns = net.ns, ld = net.ld;
   for (int kb = 0; kb < ns; kb += PANEL) {
     const int ke = min(kb + PANEL, ns), nb = ke - kb;
+    if (tid == 0) dinv[kb] = 1.0 / A[kb * ld + kb];
+    __syncthreads();
     for (int k = kb; k < ke; k++) {  // the panel: columns kb..ke-1
-      const double d = 1.0 / A[k * ld + k];
-      if (tid == 0) dinv[k] = d;
-      for (int i = k + 1 + tid; i < ns; i += nt) {
+      const double d = dinv[k];
+      for (int i = k + 1 + tid; i < ns; i += NT) {
         double* ai = A + i * ld;
         const double l = ai[k] * d;
         ai[k] = l;
         for (int j = k + 1; j < ke; j++) ai[j] = fma(-l, A[k * ld + j], ai[j]);
+        if (i == k + 1 && i < ke) dinv[i] = 1.0 / ai[i];  // the next pivot, final now
       }
       __syncthreads();
     }
     if (ke == ns) break;
     // the block's pivot rows beyond the panel: row kb + s takes pivots kb .. kb + s - 1
-    for (int j = ke + tid; j < ns; j += nt) {
+    for (int j = ke + tid; j < ns; j += NT) {
       for (int s = 1; s < nb; s++) {
         double a = A[(kb + s) * ld + j];
         for (int t = 0; t < s; t++) a = fma(-A[(kb + s) * ld + kb + t], A[(kb + t) * ld + j], a);
@@ -261,20 +313,7 @@ __device__ void lu_factor(const Net& net, double* A, double* dinv, int tid, int 
       }
     }
     __syncthreads();
-    // the trailing matrix: rank-nb update, one row per thread
-    for (int i = ke + tid; i < ns; i += nt) {
-      double l[PANEL];
-      double* ai = A + i * ld;
-#pragma unroll
-      for (int t = 0; t < PANEL; t++) l[t] = t < nb ? ai[kb + t] : 0.0;
-      for (int j = ke; j < ns; j++) {
-        double a = ai[j];
-#pragma unroll
-        for (int t = 0; t < PANEL; t++)
-          if (t < nb) a = fma(-l[t], A[(kb + t) * ld + j], a);
-        ai[j] = a;
-      }
-    }
+    trailing_update<NT>(A, ld, kb, nb, ke, ns, tid);
     __syncthreads();
   }
 }

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
       jacobian_w(net, c, ntot, tid, nt);
       for (int i = tid; i < ns; i += nt) c.A[i * ld + i] += igh;  // M0 = I / (gamma h) - Jn
       __syncthreads();
-      lu_factor(net, c.A, c.dinv, tid, nt);
+      lu_factor<32 * W>(net, c.A, c.dinv, tid);
       if (warp == 0) {  // stages 1 and 2: K1 and M0^-1 w together, then Sherman-Morrison
         for (int i = lane; i < ns; i += 32) c.K1[i] = c.F[i];
         __syncwarp();
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(32 * W) debug_try_kernel(const Net net, const 
   __syncthreads();
   for (int i = tid; i < ns; i += nt) c.A[i * ld + i] += igh;
   __syncthreads();
-  lu_factor(net, c.A, c.dinv, tid, nt);
+  lu_factor<32 * W>(net, c.A, c.dinv, tid);
   for (int e = tid; e < ns * ns; e += nt) o[e] = c.A[(e / ns) * ld + e % ns];
   o += ns * ns;
   for (int i = tid; i < ns; i += nt) o[i] = c.dinv[i];
