@@ -200,6 +200,7 @@ def main() -> None:
     ms = total_ms / args.steps
     counts = solver.count.cpu().tolist()
     nt = tries.cpu().tolist()
+    phases = phase_shares(solver, lib, x, T, P, dt, h, J, dev)
     steps_mean = float(out["steps"].mean())
     value = world * B / (ms * 1e-3)
     # roofline: algorithmic FP64 work of the call kernel per launch / its time (events on the launching stream)
@@ -217,7 +218,8 @@ def main() -> None:
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
                    "accepted_steps_mean": steps_mean, "tries_per_cell": nt[0] / args.steps / B,
                    "retries_per_cell": nt[1] / args.steps / B, "recovery_tries": nt[2] / args.steps,
-                   "counts": dict(zip(["queue", *abi_counts()], counts)), "spinup": spin, "layout": solver.info},
+                   "counts": dict(zip(["queue", *abi_counts()], counts)), "spinup": spin, "layout": solver.info,
+                   "phase_shares": phases},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak / 1e3, "unit": "TFLOP/s",
                      "frac": achieved / (peak / 1e3) if peak else None, "traffic": None,
                      "peak_source": "measured in-process: FP64 fma chains on every SM (mx_probe_fp64)",
@@ -234,6 +236,22 @@ def main() -> None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+PHASES = ("rates", "rhs_jacobian", "lu", "stages12", "stage3", "stage4", "control", "output_guard")
+
+
+def phase_shares(solver, lib, x, T, P, dt, h, J, dev) -> dict:
+    """One untimed call through the call kernel's clock64-instrumented variant: the share of SM cycles per phase."""
+    import torch
+
+    cycles = torch.zeros(8, dtype=torch.int64, device=dev)
+    lib.mx_set_phase_counter(solver._handle, cycles.data_ptr())
+    solver.launch_raw(x, T, P, dt, h, rtol=1e-3, atol=1e-25, max_steps=4000, J=J)
+    torch.cuda.synchronize(dev)
+    lib.mx_set_phase_counter(solver._handle, None)
+    c = cycles.cpu().double()
+    return {k: round(float(v), 4) for k, v in zip(PHASES, (c / c.sum()).tolist())}
 
 
 def abi_counts():

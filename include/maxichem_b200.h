@@ -142,6 +142,11 @@ int mx_debug_try(mx_solver* s, const double* x, double T, double P, double h, co
  * feeds the measured roofline (algorithmic FLOPs per try are a property of the network's tables). */
 int mx_set_try_counter(mx_solver* s, int64_t* tries);
 
+/* Register a device int64[8] that later calls add per-phase SM cycles to (clock64 on one thread per cell): rates, F
+ * and Jacobian, LU, stages 1-2, stage 3, stage 4, step control, output and guard; NULL returns to the plain kernel.
+ * No counterpart in the reference: it attributes the call kernel's time for tuning. */
+int mx_set_phase_counter(mx_solver* s, int64_t* cycles);
+
 /* FP64 fused multiply-add throughput of a device in GFLOP/s, from independent fma chains on every SM (synchronises
  * the device). No counterpart in the reference: the roofline's FP64 denominator, which the driver-measured peaks
  * file does not hold. */

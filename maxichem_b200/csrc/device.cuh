@@ -177,22 +177,26 @@ __device__ void cell_rates(const Net& net, const Cell& c, double Tc, double nd, 
 
 // ---- right-hand side (rhs, common.cuh:282-353) ----
 
-// F = (ntot / nd) S v(n) at Y, u0 = S v / nd into U when u0; n = nd Y / ntot. Returns ntot. Three barriers.
-__device__ double rhs(const Net& net, const Cell& c, const double* Y, bool u0, double nd, int tid, int nt) {
-  const int lane = tid & 31, ns = net.ns;
+// A barrier over the threads of a group: named barrier id (0 is __syncthreads' own) over n threads.
+__device__ __forceinline__ void group_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+
+// F = (ntot / nd) S v(n) at Y, u0 = S v / nd into U when u0; n = nd Y / ntot. Returns ntot. Run by a group of whole
+// warps (gtid its thread index, gnt its size, synchronised by named barrier bar); three barriers.
+__device__ double rhs(const Net& net, const Cell& c, const double* Y, bool u0, double nd, int gtid, int gnt, int bar) {
+  const int lane = gtid & 31, ns = net.ns;
   const double ntot = lane_sum(Y, ns, lane), xf = nd / ntot, ixf = ntot / nd;
-  for (int i = tid; i < ns; i += nt) c.n[i] = Y[i] * xf;
-  if (tid == 0) c.n[ns] = 1.0;
-  __syncthreads();
+  for (int i = gtid; i < ns; i += gnt) c.n[i] = Y[i] * xf;
+  if (gtid == 0) c.n[ns] = 1.0;
+  group_sync(bar, gnt);
   const double* n = c.n;
-  for (int r = tid; r < net.nr; r += nt) {
+  for (int r = gtid; r < net.nr; r += gnt) {
     const uint64_t w = __ldg(net.rx8 + r);
     const double a = c.kf[r] * n[w & 255] * n[(w >> 8) & 255] * n[(w >> 16) & 255];
     const double b = c.kr[r] * n[(w >> 24) & 255] * n[(w >> 32) & 255] * n[(w >> 40) & 255];
     c.v[r] = a - b;
   }
-  __syncthreads();
-  for (int i = tid; i < ns; i += nt) {
+  group_sync(bar, gnt);
+  for (int i = gtid; i < ns; i += gnt) {
     double s = 0.0;
     const int t1 = __ldg(net.sv_ptr + i + 1);
     for (int t = __ldg(net.sv_ptr + i); t < t1; t++) {
@@ -202,8 +206,13 @@ __device__ double rhs(const Net& net, const Cell& c, const double* Y, bool u0, d
     c.F[i] = s * ixf;
     if (u0) c.U[i] = s / nd;
   }
-  __syncthreads();
+  group_sync(bar, gnt);
   return ntot;
+}
+
+__device__ __forceinline__ double rhs(const Net& net, const Cell& c, const double* Y, bool u0, double nd, int tid,
+                                      int nt) {
+  return rhs(net, c, Y, u0, nd, tid, nt, 0);
 }
 
 // A = -Jn (dense, row stride ld), then U = u0 + (-Jn N) / ntot (call.cuh:61-79, jacobian_times_x). Three barriers.
@@ -329,7 +338,10 @@ __device__ __forceinline__ double pick(const double (&a)[R], int idx) {
 }
 
 // y <- M0^-1 y on one warp for NV vectors (1 or 2) with the factors of lu_factor: lane l holds rows l + 32 p.
-// Forward unit L in ascending k, U in descending k with x_k = a_k / U_kk (msolve, common.cuh:504-522).
+// Forward unit L in ascending k, U in descending k with x_k = a_k / U_kk (msolve, common.cuh:504-522), four pivots
+// per round: the four pivot rows' current values are broadcast at once and every lane finishes those four itself
+// (a 4 x 4 triangle), then updates its own rows with the four in order. Each entry receives the same fma's in the
+// same order as the one-pivot sweep, so the bits are those of the one-pivot sweep.
 template <int R, int NV>
 __device__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1, int lane) {
   const int ns = net.ns, ld = net.ld;
@@ -341,31 +353,100 @@ __device__ void lu_solve(const Net& net, const double* A, const double* dinv, do
     a[0][p] = i < ns ? y0[i] : 0.0;
     if (NV == 2) a[NV - 1][p] = i < ns ? y1[i] : 0.0;
   }
-  for (int k = 0; k < ns - 1; k++) {
-    const int src = k & 31, kp = k >> 5;
-    const double yk0 = __shfl_sync(FULL, pick<R>(a[0], kp), src);
-    const double yk1 = NV == 2 ? __shfl_sync(FULL, pick<R>(a[NV - 1], kp), src) : 0.0;
+  // forward: pivots kb .. kb + q - 1 (the last row takes no pivot of its own)
+  for (int kb = 0; kb < ns - 1; kb += 4) {
+    const int q = min(4, ns - 1 - kb);
+    double yv[NV][4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = min(kb + j, ns - 1);
+#pragma unroll
+      for (int v = 0; v < NV; v++) yv[v][j] = __shfl_sync(FULL, pick<R>(a[v], k >> 5), k & 31);
+    }
+    double lt[6];  // L[kb+1][kb], L[kb+2][kb], L[kb+2][kb+1], L[kb+3][kb], L[kb+3][kb+1], L[kb+3][kb+2]
+    lt[0] = q > 1 ? A[(kb + 1) * ld + kb] : 0.0;
+    lt[1] = q > 2 ? A[(kb + 2) * ld + kb] : 0.0;
+    lt[2] = q > 2 ? A[(kb + 2) * ld + kb + 1] : 0.0;
+    lt[3] = q > 3 ? A[(kb + 3) * ld + kb] : 0.0;
+    lt[4] = q > 3 ? A[(kb + 3) * ld + kb + 1] : 0.0;
+    lt[5] = q > 3 ? A[(kb + 3) * ld + kb + 2] : 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      yv[v][1] = fma(-lt[0], yv[v][0], yv[v][1]);
+      yv[v][2] = fma(-lt[2], yv[v][1], fma(-lt[1], yv[v][0], yv[v][2]));
+      yv[v][3] = fma(-lt[5], yv[v][2], fma(-lt[4], yv[v][1], fma(-lt[3], yv[v][0], yv[v][3])));
+    }
 #pragma unroll
     for (int p = 0; p < R; p++) {
       const int i = lane + 32 * p;
-      if (32 * p + 31 > k && i > k && i < ns) {
-        const double m = A[i * ld + k];
-        a[0][p] = fma(-m, yk0, a[0][p]);
-        if (NV == 2) a[NV - 1][p] = fma(-m, yk1, a[NV - 1][p]);
+      if (32 * p + 31 <= kb || i >= ns) continue;
+      if (i >= kb + q) {
+        const double* ai = A + i * ld + kb;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          if (j < q) {
+            const double m = ai[j];
+#pragma unroll
+            for (int v = 0; v < NV; v++) a[v][p] = fma(-m, yv[v][j], a[v][p]);
+          }
+        }
+      } else if (i > kb) {
+#pragma unroll
+        for (int j = 1; j < 4; j++)
+          if (i == kb + j)
+#pragma unroll
+            for (int v = 0; v < NV; v++) a[v][p] = yv[v][j];
       }
     }
   }
-  for (int k = ns - 1; k > 0; k--) {
-    const int src = k & 31, kp = k >> 5;
-    const double z0 = __shfl_sync(FULL, pick<R>(a[0], kp) * pick<R>(d, kp), src);
-    const double z1 = NV == 2 ? __shfl_sync(FULL, pick<R>(a[NV - 1], kp) * pick<R>(d, kp), src) : 0.0;
+  // backward: pivots hi, hi - 1, .., lo (descending), x_k = a_k d_k; rows below lo take them in that order
+  for (int hi = ns - 1; hi > 0; hi -= 4) {
+    const int lo = max(hi - 3, 1), q = hi - lo + 1;
+    double av[NV][4], dv[4], ut[6];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = max(hi - j, 0);
+#pragma unroll
+      for (int v = 0; v < NV; v++) av[v][j] = __shfl_sync(FULL, pick<R>(a[v], k >> 5), k & 31);
+      dv[j] = dinv[k];
+    }
+    // U[hi-1][hi], U[hi-2][hi], U[hi-2][hi-1], U[hi-3][hi], U[hi-3][hi-1], U[hi-3][hi-2]
+    ut[0] = q > 1 ? A[(hi - 1) * ld + hi] : 0.0;
+    ut[1] = q > 2 ? A[(hi - 2) * ld + hi] : 0.0;
+    ut[2] = q > 2 ? A[(hi - 2) * ld + hi - 1] : 0.0;
+    ut[3] = q > 3 ? A[(hi - 3) * ld + hi] : 0.0;
+    ut[4] = q > 3 ? A[(hi - 3) * ld + hi - 1] : 0.0;
+    ut[5] = q > 3 ? A[(hi - 3) * ld + hi - 2] : 0.0;
+    double z[NV][4];
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      z[v][0] = av[v][0] * dv[0];
+      av[v][1] = fma(-ut[0], z[v][0], av[v][1]);
+      z[v][1] = av[v][1] * dv[1];
+      av[v][2] = fma(-ut[2], z[v][1], fma(-ut[1], z[v][0], av[v][2]));
+      z[v][2] = av[v][2] * dv[2];
+      av[v][3] = fma(-ut[5], z[v][2], fma(-ut[4], z[v][1], fma(-ut[3], z[v][0], av[v][3])));
+      z[v][3] = av[v][3] * dv[3];
+    }
 #pragma unroll
     for (int p = 0; p < R; p++) {
       const int i = lane + 32 * p;
-      if (32 * p < k && i < k) {
-        const double m = A[i * ld + k];
-        a[0][p] = fma(-m, z0, a[0][p]);
-        if (NV == 2) a[NV - 1][p] = fma(-m, z1, a[NV - 1][p]);
+      if (32 * p >= hi || i >= ns) continue;
+      if (i < lo) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          if (j < q) {
+            const double m = A[i * ld + hi - j];
+#pragma unroll
+            for (int v = 0; v < NV; v++) a[v][p] = fma(-m, z[v][j], a[v][p]);
+          }
+        }
+      } else if (i < hi) {
+#pragma unroll
+        for (int j = 1; j < 4; j++)
+          if (i == hi - j)
+#pragma unroll
+            for (int v = 0; v < NV; v++) a[v][p] = av[v][j];
       }
     }
   }

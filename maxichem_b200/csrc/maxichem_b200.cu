@@ -22,12 +22,29 @@ namespace {
 
 constexpr int WARPS = 4;  // warps per cell
 
+// Phases of a try that the profiling variant of the call kernel times (clock64 on thread 0, summed over cells).
+enum { PH_RATES, PH_RHS_JAC, PH_LU, PH_STAGE12, PH_STAGE3, PH_STAGE4, PH_CONTROL, PH_OUTPUT, PH_COUNT };
+
 // The call kernel: screening, rates, Rodas3 steps, output and the guard, per cell (call.cuh:5-177, guard.cuh:114-140).
-template <int W, int R>
-__global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallArgs a) {
+// PROF: also sum clock64 cycles per phase into prof[PH_COUNT].
+template <int W, int R, bool PROF>
+__global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallArgs a, long long* prof) {
   extern __shared__ double smem[];
   const Cell c = cell_arrays(net, smem);
   const int tid = (int)threadIdx.x, nt = 32 * W, lane = tid & 31, warp = tid >> 5, ns = net.ns, ld = net.ld;
+  long long ph[PH_COUNT], t0 = 0;
+  if (PROF) {
+#pragma unroll
+    for (int q = 0; q < PH_COUNT; q++) ph[q] = 0;
+    t0 = clock64();
+  }
+  auto mark = [&](int q) {
+    if (PROF && tid == 0) {
+      const long long t = clock64();
+      ph[q] += t - t0;
+      t0 = t;
+    }
+  };
   int cell = (int)blockIdx.x;
   while (cell < a.B) {
     const double Tc = a.T[cell], dt = a.dt[cell], hin = a.h_in[cell];
@@ -51,7 +68,8 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
       const double ps = warp_sum(p), mxv = warp_max(pm);
       const bool forcing = isfinite(Tc) && isfinite(nd) && nd > 0.0 && isfinite(dt) && dt >= 0.0;
       const bool fine = fabs(ps - 1.0) <= MX_X_SUM_TOL && mxv > 0.0 && forcing;
-      const int st = Tc < MX_T_MIN ? MX_REFUSED_COLD : (Tc > MX_T_MAX ? MX_REFUSED_HOT : (fine ? 0 : MX_REFUSED_BAD_INPUT));
+      const int st =
+          Tc < MX_T_MIN ? MX_REFUSED_COLD : (Tc > MX_T_MAX ? MX_REFUSED_HOT : (fine ? 0 : MX_REFUSED_BAD_INPUT));
       if (lane == 0) {
         c.ints[0] = st;
         a.status[cell] = st;
@@ -61,6 +79,7 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
     __syncthreads();
     const int st = c.ints[0];
     if (st == 0) cell_rates(net, c, Tc, nd, Jc, tid, nt);
+    mark(PH_RATES);
     const double h0 = isfinite(hin) ? hin : dt;  // a non-finite h acts as dt
     StepState s = {fmax(fmin(h0, dt), MX_H_MIN), 0.0, 0.0, 0.0, 0.0, false};
     int it = (dt > 0.0 && st == 0) ? 0 : a.max_steps;  // a refused cell takes no step
@@ -75,21 +94,30 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
       jacobian_w(net, c, ntot, tid, nt);
       for (int i = tid; i < ns; i += nt) c.A[i * ld + i] += igh;  // M0 = I / (gamma h) - Jn
       __syncthreads();
+      mark(PH_RHS_JAC);
       lu_factor<32 * W>(net, c.A, c.dinv, tid);
-      if (warp == 0) {  // stages 1 and 2: K1 and M0^-1 w together, then Sherman-Morrison
+      mark(PH_LU);
+      if (warp == 0) {  // stage 1: K1 and M0^-1 w together, then Sherman-Morrison
         for (int i = lane; i < ns; i += 32) c.K1[i] = c.F[i];
         __syncwarp();
         lu_solve<R, 2>(net, c.A, c.dinv, c.K1, c.U, lane);
         c0 = 1.0 / (1.0 - lane_sum(c.U, ns, lane));
         sherman(net, c.K1, c.U, c0, lane);
-        for (int i = lane; i < ns; i += 32) c.K2[i] = fma(RODAS_C21 * ih, c.K1[i], c.F[i]);
-        __syncwarp();
-        lu_solve<R, 1>(net, c.A, c.dinv, c.K2, nullptr, lane);
-        sherman(net, c.K2, c.U, c0, lane);
-        for (int i = lane; i < ns; i += 32) c.Y[i] = c.N[i] + 2.0 * c.K1[i];
       }
       __syncthreads();
-      rhs(net, c, c.Y, false, nd, tid, nt);
+      for (int i = tid; i < ns; i += nt) {
+        c.K2[i] = fma(RODAS_C21 * ih, c.K1[i], c.F[i]);
+        c.Y[i] = c.N[i] + 2.0 * c.K1[i];
+      }
+      __syncthreads();
+      if (warp == 0) {  // stage 2 on warp 0 while the other warps evaluate F(Y3), Y3 = N + 2 K1
+        lu_solve<R, 1>(net, c.A, c.dinv, c.K2, nullptr, lane);
+        sherman(net, c.K2, c.U, c0, lane);
+      } else {
+        rhs(net, c, c.Y, false, nd, tid - 32, nt - 32, 1);
+      }
+      __syncthreads();
+      mark(PH_STAGE12);
       if (warp == 0) {  // stage 3
         for (int i = lane; i < ns; i += 32) c.K3[i] = fma(ih, c.K1[i] - c.K2[i], c.F[i]);
         __syncwarp();
@@ -99,6 +127,7 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
       }
       __syncthreads();
       rhs(net, c, c.Y, false, nd, tid, nt);
+      mark(PH_STAGE3);
       if (warp == 0) {  // stage 4 and the error
         for (int i = lane; i < ns; i += 32)
           c.K4[i] = fma(ih, fma(-RODAS_C43, c.K3[i], c.K1[i] - c.K2[i]), c.F[i]);
@@ -108,6 +137,7 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
         try_error(net, c, s.t == 0.0, a.rtol, a.atol, lane);
       }
       __syncthreads();
+      mark(PH_STAGE4);
       const double en = c.red[0];
       const bool ok = c.red[1] != 0.0;
       if (ok) {
@@ -122,6 +152,7 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
       s.pha = ha;
       it++;
       __syncthreads();
+      mark(PH_CONTROL);
     }
     // x = N / sum N in the network's order (write_state), then the guard on it (check_cell)
     if (warp == 0) {
@@ -166,6 +197,11 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
     for (int i = tid; i < ns; i += nt) xo[i] = c.Y[i];
     cell = c.ints[1];
     __syncthreads();
+    mark(PH_OUTPUT);
+  }
+  if (PROF && tid == 0) {
+#pragma unroll
+    for (int q = 0; q < PH_COUNT; q++) atomicAdd((unsigned long long*)prof + q, (unsigned long long)ph[q]);
   }
 }
 
@@ -404,26 +440,27 @@ __global__ void add_counts_kernel(const int* count, long long* total) {
   if (i < MX_COUNT_SLOTS) total[i] += count[i];
 }
 
-typedef void (*CallFn)(const Net, const CallArgs);
+typedef void (*CallFn)(const Net, const CallArgs, long long*);
 typedef void (*DebugFn)(const Net, const double*, double, double, double, const double*, double, double, double*);
 typedef void (*RecoverFn)(const Net, const CallArgs, int);
 
 
 template <int R>
-void kernels_for(CallFn* call, RecoverFn* rec, DebugFn* dbg) {
-  *call = call_kernel<WARPS, R>;
+void kernels_for(CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg) {
+  *call = call_kernel<WARPS, R, false>;
+  *prof = call_kernel<WARPS, R, true>;
   *rec = recover_kernel<WARPS, R>;
   *dbg = debug_try_kernel<WARPS, R>;
 }
 
 // rows per lane of the warp solves: species up to 32, 64, 96, 128, 256
-bool pick_kernels(int ns, CallFn* call, RecoverFn* rec, DebugFn* dbg, int* r) {
+bool pick_kernels(int ns, CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg, int* r) {
   const int need = (ns + 31) / 32;
-  if (need <= 1) { kernels_for<1>(call, rec, dbg); *r = 1; return true; }
-  if (need <= 2) { kernels_for<2>(call, rec, dbg); *r = 2; return true; }
-  if (need <= 3) { kernels_for<3>(call, rec, dbg); *r = 3; return true; }
-  if (need <= 4) { kernels_for<4>(call, rec, dbg); *r = 4; return true; }
-  if (need <= 8) { kernels_for<8>(call, rec, dbg); *r = 8; return true; }
+  if (need <= 1) { kernels_for<1>(call, prof, rec, dbg); *r = 1; return true; }
+  if (need <= 2) { kernels_for<2>(call, prof, rec, dbg); *r = 2; return true; }
+  if (need <= 3) { kernels_for<3>(call, prof, rec, dbg); *r = 3; return true; }
+  if (need <= 4) { kernels_for<4>(call, prof, rec, dbg); *r = 4; return true; }
+  if (need <= 8) { kernels_for<8>(call, prof, rec, dbg); *r = 8; return true; }
   return false;
 }
 
@@ -456,6 +493,7 @@ struct mx_solver {
   Net net{};
   std::vector<void*> buffers;
   CallFn call = nullptr;
+  CallFn call_prof = nullptr;
   RecoverFn recover = nullptr;
   DebugFn debug = nullptr;
   int rows_per_lane = 0;
@@ -464,6 +502,7 @@ struct mx_solver {
   int* list = nullptr;
   int64_t list_capacity = 0;
   unsigned long long* tries = nullptr;
+  long long* phases = nullptr;
 };
 
 namespace {
@@ -524,7 +563,7 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   double etot = 0.0;
   for (int i = 0; i < ns * n->nel; i++) etot += n->atoms[i];
   net.etot = etot;
-  if (!pick_kernels(ns, &s->call, &s->recover, &s->debug, &s->rows_per_lane)) {
+  if (!pick_kernels(ns, &s->call, &s->call_prof, &s->recover, &s->debug, &s->rows_per_lane)) {
     delete s;
     return MX_ERR_NETWORK;
   }
@@ -567,6 +606,8 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
     e = cudaFuncSetAttribute((const void*)s->recover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)s->debug, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)s->call_prof, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->call_ctas, (const void*)s->call, 32 * WARPS, s->smem);
   if (e == cudaSuccess)
@@ -649,7 +690,10 @@ extern "C" int mx_call(mx_solver* s, const double* x, const double* T, const dou
     CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status, count,
                s->list, s->tries};
     const int grid = (int)std::min<int64_t>(B, (int64_t)s->call_ctas * s->sms);
-    s->call<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a);
+    if (s->phases)
+      s->call_prof<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, s->phases);
+    else
+      s->call<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, nullptr);
     const int rgrid = (int)std::min<int64_t>(B, (int64_t)s->recover_ctas * s->sms);
     s->recover<<<rgrid, 32 * WARPS, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
     e = cudaGetLastError();
@@ -716,6 +760,12 @@ extern "C" int mx_debug_try(mx_solver* s, const double* x, double T, double P, d
   DeviceScope scope(s->device);
   s->debug<<<1, 32 * WARPS, s->smem, (cudaStream_t)stream>>>(s->net, x, T, P, h, J, rtol, atol, out);
   return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
+}
+
+extern "C" int mx_set_phase_counter(mx_solver* s, int64_t* cycles) {
+  if (!s) return MX_ERR_CLOSED;
+  s->phases = (long long*)cycles;
+  return MX_OK;
 }
 
 extern "C" int mx_set_try_counter(mx_solver* s, int64_t* tries) {
