@@ -147,6 +147,12 @@ int mx_set_try_counter(mx_solver* s, int64_t* tries);
  * No counterpart in the reference: it attributes the call kernel's time for tuning. */
 int mx_set_phase_counter(mx_solver* s, int64_t* cycles);
 
+/* Average SM cycles of each device function of one try, each repeated reps times on one cell in each of ctas CTAs
+ * (device x [ns], J [nj]): rates, F, Jacobian and w, LU, two-vector solve, one-vector solve, Sherman-Morrison, error,
+ * guard test, into the device int64[9] cycles. No counterpart in the reference: a tuning hook. */
+int mx_time_phases(mx_solver* s, const double* x, double T, double P, double h, const double* J, int32_t reps,
+                   int32_t ctas, int64_t* cycles, void* stream);
+
 /* FP64 fused multiply-add throughput of a device in GFLOP/s, from independent fma chains on every SM (synchronises
  * the device). No counterpart in the reference: the roofline's FP64 denominator, which the driver-measured peaks
  * file does not hold. */

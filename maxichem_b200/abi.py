@@ -87,6 +87,10 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "mx_destroy": (ctypes.c_int, [_P]),
     "mx_set_try_counter": (ctypes.c_int, [_P, _P]),
     "mx_set_phase_counter": (ctypes.c_int, [_P, _P]),
+    "mx_time_phases": (
+        ctypes.c_int,
+        [_P, _P, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, ctypes.c_int32, ctypes.c_int32, _P, _P],
+    ),
     "mx_debug_try": (
         ctypes.c_int,
         [_P, _P, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, ctypes.c_double, ctypes.c_double, _P, _P],

@@ -408,6 +408,67 @@ __global__ void __launch_bounds__(32 * W) debug_try_kernel(const Net net, const 
   }
 }
 
+// Cycles of each device function of a try, repeated reps times on one cell in every CTA (a tuning hook): rates,
+// F, Jacobian and w, LU, two-vector solve, one-vector solve, Sherman-Morrison, error, guard test. cycles[9] receives
+// the CTA-0 averages.
+template <int W, int R>
+__global__ void __launch_bounds__(32 * W) time_phases_kernel(const Net net, const double* x0, double Tc, double P,
+                                                             double ha, const double* Jc, int reps,
+                                                             long long* cycles) {
+  extern __shared__ double smem[];
+  const Cell c = cell_arrays(net, smem);
+  const int tid = (int)threadIdx.x, nt = 32 * W, lane = tid & 31, warp = tid >> 5, ns = net.ns, ld = net.ld;
+  const double nd = P / (MX_KB * Tc), igh = 1.0 / (GAMMA * ha);
+  long long acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = tid; i < ns; i += nt) c.N[i] = x0[__ldg(net.perm + i)];
+  __syncthreads();
+  for (int r = 0; r < reps; r++) {
+    long long t = clock64();
+    cell_rates(net, c, Tc, nd, Jc, tid, nt);
+    long long u = clock64();
+    acc[0] += u - t;
+    const double ntot = rhs(net, c, c.N, true, nd, tid, nt);
+    t = clock64();
+    acc[1] += t - u;
+    jacobian_w(net, c, ntot, tid, nt);
+    for (int i = tid; i < ns; i += nt) c.A[i * ld + i] += igh;
+    __syncthreads();
+    u = clock64();
+    acc[2] += u - t;
+    lu_factor<32 * W>(net, c.A, c.dinv, tid);
+    t = clock64();
+    acc[3] += t - u;
+    if (warp == 0) {
+      for (int i = lane; i < ns; i += 32) c.K1[i] = c.F[i];
+      __syncwarp();
+      u = clock64();
+      lu_solve<R, 2>(net, c.A, c.dinv, c.K1, c.U, lane);
+      t = clock64();
+      acc[4] += t - u;
+      lu_solve<R, 1>(net, c.A, c.dinv, c.K2, nullptr, lane);
+      u = clock64();
+      acc[5] += u - t;
+      sherman(net, c.K2, c.U, 0.5, lane);
+      t = clock64();
+      acc[6] += t - u;
+      try_error(net, c, true, 1e-3, 1e-25, lane);
+      u = clock64();
+      acc[7] += u - t;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int i = 0; i < ns; i++) c.Y[__ldg(net.perm + i)] = c.N[i];
+      t = clock64();
+      check_cell(net, x0, c.Y, 1, 1.0, 1e-25);
+      u = clock64();
+      acc[8] += u - t;
+    }
+    __syncthreads();
+  }
+  if (blockIdx.x == 0 && tid == 0)
+    for (int q = 0; q < 9; q++) cycles[q] = acc[q] / reps;
+}
+
 // The guard alone, one thread per cell (guard.cuh:114-140), on results in global memory.
 __global__ void guard_kernel(const Net net, const double* x0, double* xout, const int* done, const double* nok,
                              const int* status, int B, double atol, int* flag, int* count, int* list) {
@@ -443,10 +504,12 @@ __global__ void add_counts_kernel(const int* count, long long* total) {
 typedef void (*CallFn)(const Net, const CallArgs, long long*);
 typedef void (*DebugFn)(const Net, const double*, double, double, double, const double*, double, double, double*);
 typedef void (*RecoverFn)(const Net, const CallArgs, int);
+typedef void (*TimeFn)(const Net, const double*, double, double, double, const double*, int, long long*);
 
 
 template <int R>
-void kernels_for(CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg) {
+void kernels_for(CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg, TimeFn* tim) {
+  *tim = time_phases_kernel<WARPS, R>;
   *call = call_kernel<WARPS, R, false>;
   *prof = call_kernel<WARPS, R, true>;
   *rec = recover_kernel<WARPS, R>;
@@ -454,13 +517,13 @@ void kernels_for(CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg) {
 }
 
 // rows per lane of the warp solves: species up to 32, 64, 96, 128, 256
-bool pick_kernels(int ns, CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg, int* r) {
+bool pick_kernels(int ns, CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg, TimeFn* tim, int* r) {
   const int need = (ns + 31) / 32;
-  if (need <= 1) { kernels_for<1>(call, prof, rec, dbg); *r = 1; return true; }
-  if (need <= 2) { kernels_for<2>(call, prof, rec, dbg); *r = 2; return true; }
-  if (need <= 3) { kernels_for<3>(call, prof, rec, dbg); *r = 3; return true; }
-  if (need <= 4) { kernels_for<4>(call, prof, rec, dbg); *r = 4; return true; }
-  if (need <= 8) { kernels_for<8>(call, prof, rec, dbg); *r = 8; return true; }
+  if (need <= 1) { kernels_for<1>(call, prof, rec, dbg, tim); *r = 1; return true; }
+  if (need <= 2) { kernels_for<2>(call, prof, rec, dbg, tim); *r = 2; return true; }
+  if (need <= 3) { kernels_for<3>(call, prof, rec, dbg, tim); *r = 3; return true; }
+  if (need <= 4) { kernels_for<4>(call, prof, rec, dbg, tim); *r = 4; return true; }
+  if (need <= 8) { kernels_for<8>(call, prof, rec, dbg, tim); *r = 8; return true; }
   return false;
 }
 
@@ -496,6 +559,7 @@ struct mx_solver {
   CallFn call_prof = nullptr;
   RecoverFn recover = nullptr;
   DebugFn debug = nullptr;
+  TimeFn timer = nullptr;
   int rows_per_lane = 0;
   size_t smem = 0;
   int sms = 0, call_ctas = 0, recover_ctas = 0;
@@ -563,7 +627,7 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   double etot = 0.0;
   for (int i = 0; i < ns * n->nel; i++) etot += n->atoms[i];
   net.etot = etot;
-  if (!pick_kernels(ns, &s->call, &s->call_prof, &s->recover, &s->debug, &s->rows_per_lane)) {
+  if (!pick_kernels(ns, &s->call, &s->call_prof, &s->recover, &s->debug, &s->timer, &s->rows_per_lane)) {
     delete s;
     return MX_ERR_NETWORK;
   }
@@ -606,6 +670,8 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
     e = cudaFuncSetAttribute((const void*)s->recover, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)s->debug, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)s->timer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)s->call_prof, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
@@ -759,6 +825,14 @@ extern "C" int mx_debug_try(mx_solver* s, const double* x, double T, double P, d
   if (!s || !x || !out || (s->net.nj > 0 && !J)) return MX_ERR_ARGUMENT;
   DeviceScope scope(s->device);
   s->debug<<<1, 32 * WARPS, s->smem, (cudaStream_t)stream>>>(s->net, x, T, P, h, J, rtol, atol, out);
+  return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
+}
+
+extern "C" int mx_time_phases(mx_solver* s, const double* x, double T, double P, double h, const double* J,
+                              int32_t reps, int32_t ctas, int64_t* cycles, void* stream) {
+  if (!s || !x || !cycles || reps < 1 || ctas < 1 || (s->net.nj > 0 && !J)) return MX_ERR_ARGUMENT;
+  DeviceScope scope(s->device);
+  s->timer<<<ctas, 32 * WARPS, s->smem, (cudaStream_t)stream>>>(s->net, x, T, P, h, J, reps, (long long*)cycles);
   return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
