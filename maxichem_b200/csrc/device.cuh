@@ -138,7 +138,7 @@ __device__ __forceinline__ double gibbs_rt(const double* __restrict__ a, double 
 }
 
 // kf, kr of one cell (cell_rates, common.cuh:222-242); g (ns + 1 doubles) is scratch. Two barriers.
-__device__ void cell_rates(const Net& net, const Cell& c, double Tc, double nd, const double* __restrict__ Jc,
+__device__ __forceinline__ void cell_rates(const Net& net, const Cell& c, double Tc, double nd, const double* __restrict__ Jc,
                            int tid, int nt) {
   const double lT = log(Tc), iT = 1.0 / Tc, lKT = log(MX_KB * Tc / MX_P0);
   double* g = c.v;
@@ -182,7 +182,7 @@ __device__ __forceinline__ void group_sync(int id, int n) { asm volatile("bar.sy
 
 // F = (ntot / nd) S v(n) at Y, u0 = S v / nd into U when u0; n = nd Y / ntot. Returns ntot. Run by a group of whole
 // warps (gtid its thread index, gnt its size, synchronised by named barrier bar); three barriers.
-__device__ double rhs(const Net& net, const Cell& c, const double* Y, bool u0, double nd, int gtid, int gnt, int bar) {
+__device__ __forceinline__ double rhs(const Net& net, const Cell& c, const double* Y, bool u0, double nd, int gtid, int gnt, int bar) {
   const int lane = gtid & 31, ns = net.ns;
   const double ntot = lane_sum(Y, ns, lane), xf = nd / ntot, ixf = ntot / nd;
   for (int i = gtid; i < ns; i += gnt) c.n[i] = Y[i] * xf;
@@ -216,7 +216,7 @@ __device__ __forceinline__ double rhs(const Net& net, const Cell& c, const doubl
 }
 
 // A = -Jn (dense, row stride ld), then U = u0 + (-Jn N) / ntot (call.cuh:61-79, jacobian_times_x). Three barriers.
-__device__ void jacobian_w(const Net& net, const Cell& c, double ntot, int tid, int nt) {
+__device__ __forceinline__ void jacobian_w(const Net& net, const Cell& c, double ntot, int tid, int nt) {
   const int ns = net.ns, ld = net.ld;
   for (int i = tid; i < ns * ld; i += nt) c.A[i] = 0.0;
   __syncthreads();
@@ -295,7 +295,7 @@ __device__ __forceinline__ void trailing_update(double* A, int ld, int kb, int n
 }
 
 template <int NT>
-__device__ void lu_factor(const Net& net, double* A, double* dinv, int tid) {
+__device__ __forceinline__ void lu_factor(const Net& net, double* A, double* dinv, int tid) {
   const int ns = net.ns, ld = net.ld;
   for (int kb = 0; kb < ns; kb += PANEL) {
     const int ke = min(kb + PANEL, ns), nb = ke - kb;
@@ -343,7 +343,7 @@ __device__ __forceinline__ double pick(const double (&a)[R], int idx) {
 // (a 4 x 4 triangle), then updates its own rows with the four in order. Each entry receives the same fma's in the
 // same order as the one-pivot sweep, so the bits are those of the one-pivot sweep.
 template <int R, int NV>
-__device__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1, int lane) {
+__device__ __forceinline__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1, int lane) {
   const int ns = net.ns, ld = net.ld;
   double a[NV][R], d[R];
 #pragma unroll
@@ -378,24 +378,22 @@ __device__ void lu_solve(const Net& net, const double* A, const double* dinv, do
     }
 #pragma unroll
     for (int p = 0; p < R; p++) {
+      if (32 * p + 31 <= kb) continue;  // the whole block of rows is final (warp-uniform)
       const int i = lane + 32 * p;
-      if (32 * p + 31 <= kb || i >= ns) continue;
-      if (i >= kb + q) {
-        const double* ai = A + i * ld + kb;
+      const bool upd = i >= kb + q && i < ns;
+      const double* ai = A + min(i, ns - 1) * ld + kb;  // a valid row whether or not this one is updated
+      double m[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          if (j < q) {
-            const double m = ai[j];
+      for (int j = 0; j < 4; j++) m[j] = j < q ? ai[j] : 0.0;
 #pragma unroll
-            for (int v = 0; v < NV; v++) a[v][p] = fma(-m, yv[v][j], a[v][p]);
-          }
-        }
-      } else if (i > kb) {
+      for (int v = 0; v < NV; v++) {
+        double t = a[v][p];
 #pragma unroll
-        for (int j = 1; j < 4; j++)
-          if (i == kb + j)
-#pragma unroll
-            for (int v = 0; v < NV; v++) a[v][p] = yv[v][j];
+        for (int j = 0; j < 4; j++)
+          if (j < q) t = fma(-m[j], yv[v][j], t);
+        // rows kb+1 .. kb+q-1 take the values finished above; rows at or before kb keep theirs
+        const double fin = i == kb + 1 ? yv[v][1] : (i == kb + 2 ? yv[v][2] : (i == kb + 3 ? yv[v][3] : a[v][p]));
+        a[v][p] = upd ? t : fin;
       }
     }
   }
@@ -430,23 +428,22 @@ __device__ void lu_solve(const Net& net, const double* A, const double* dinv, do
     }
 #pragma unroll
     for (int p = 0; p < R; p++) {
+      if (32 * p >= hi) continue;  // every row of the block is at or after hi (warp-uniform)
       const int i = lane + 32 * p;
-      if (32 * p >= hi || i >= ns) continue;
-      if (i < lo) {
+      const bool upd = i < lo;
+      const double* ai = A + min(i, ns - 1) * ld;
+      double m[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          if (j < q) {
-            const double m = A[i * ld + hi - j];
+      for (int j = 0; j < 4; j++) m[j] = j < q ? ai[hi - j] : 0.0;
 #pragma unroll
-            for (int v = 0; v < NV; v++) a[v][p] = fma(-m, z[v][j], a[v][p]);
-          }
-        }
-      } else if (i < hi) {
+      for (int v = 0; v < NV; v++) {
+        double t = a[v][p];
 #pragma unroll
-        for (int j = 1; j < 4; j++)
-          if (i == hi - j)
-#pragma unroll
-            for (int v = 0; v < NV; v++) a[v][p] = av[v][j];
+        for (int j = 0; j < 4; j++)
+          if (j < q) t = fma(-m[j], z[v][j], t);
+        // rows lo .. hi-1 take the values finished above; rows from hi on keep theirs
+        const double fin = i == hi - 1 ? av[v][1] : (i == hi - 2 ? av[v][2] : (i == hi - 3 ? av[v][3] : a[v][p]));
+        a[v][p] = upd ? t : fin;
       }
     }
   }
@@ -471,7 +468,7 @@ __device__ __forceinline__ void sherman(const Net& net, double* y, const double*
 
 // ---- the recovery's dense LU with threshold partial pivoting (recover.cuh:7-82), on one warp ----
 
-__device__ void dense_lu_pivot(const Net& net, double* A, double* dinv, int* pr, int lane) {
+__device__ __forceinline__ void dense_lu_pivot(const Net& net, double* A, double* dinv, int* pr, int lane) {
   const int ns = net.ns, ld = net.ld;
   for (int i = lane; i < ns; i += 32) pr[i] = i;
   __syncwarp();
@@ -521,7 +518,7 @@ __device__ void dense_lu_pivot(const Net& net, double* A, double* dinv, int* pr,
 }
 
 template <int R>
-__device__ void dense_solve(const Net& net, const double* A, const double* dinv, const int* pr, double* y, int lane) {
+__device__ __forceinline__ void dense_solve(const Net& net, const double* A, const double* dinv, const int* pr, double* y, int lane) {
   const int ns = net.ns, ld = net.ld;
   double a[R], d[R];
 #pragma unroll
@@ -598,83 +595,107 @@ __device__ void try_error(const Net& net, const Cell& c, bool first, double rtol
   }
 }
 
-// ---- the guard's test (guard.cuh:13-108), on one thread ----
+// ---- the guard's test (guard.cuh:13-108), on one warp ----
+// Sums over species are formed as a warp forms them: lane l adds species l, l + 32, ... in order, then the butterfly.
+// The small element system (at most MX_MAX_ELEMENTS) is factored by every lane alike from the butterflied sums.
 
-__device__ void element_multipliers(int ns, int nel, const double* q, const double* __restrict__ atoms,
-                                    const double* e0, const double* e1, double r, double* lam) {
-  double m[MX_MAX_ELEMENTS * MX_MAX_ELEMENTS], m0[MX_MAX_ELEMENTS], y[MX_MAX_ELEMENTS];
-  for (int e = 0; e < nel * nel; e++) m[e] = 0.0;
-  for (int i = 0; i < ns; i++) {
-    const double* ai = atoms + i * nel;
-    for (int e = 0; e < nel; e++) {
-      if (ai[e] == 0.0) continue;
-      for (int f = e; f < nel; f++)
-        if (ai[f] != 0.0) m[e * nel + f] = fma(ai[e] * ai[f], q[i], m[e * nel + f]);
+// sum over species of f(i) in the warp's order (every lane returns it)
+template <typename F>
+__device__ __forceinline__ double species_sum(int ns, int lane, F f) {
+  double p = 0.0;
+  for (int i = lane; i < ns; i += 32) p = f(i, p);
+  return warp_sum(p);
+}
+
+// Guard bits of a stepped cell's result xo (network order, shared memory) against its input x0; a passing result
+// has its element shares put back in place (check_cell): x' = x (1 + sum_e lambda_e a_ie), clamped, renormalised.
+// Every lane of the warp returns the bits.
+__device__ __noinline__ int check_cell(const Net& net, const double* __restrict__ x0, double* xo, int done, double nok,
+                                       double atol, int lane) {
+  const int ns = net.ns, nel = net.nel;
+  const double* __restrict__ at = net.atoms;
+  double e0[MX_MAX_ELEMENTS], e1[MX_MAX_ELEMENTS];
+  double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+  for (int e = 0; e < MX_MAX_ELEMENTS; e++) {
+    e0[e] = e1[e] = 0.0;
+    if (e < nel) {
+      e0[e] = species_sum(ns, lane, [&](int i, double p) { return fma(__ldg(at + i * nel + e), x0[i], p); });
+      e1[e] = species_sum(ns, lane, [&](int i, double p) { return fma(__ldg(at + i * nel + e), xo[i], p); });
+      s0 += e0[e];
+      s1 += e1[e];
     }
   }
-  for (int e = 0; e < nel; e++) {
-    m0[e] = m[e * nel + e];
-    y[e] = fma(e0[e], r, -e1[e]);
+  bool fin = true;
+  for (int i = lane; i < ns; i += 32) fin = fin && isfinite(xo[i]);
+  const bool xfin = __all_sync(FULL, fin);
+  bool drift = false;
+#pragma unroll
+  for (int e = 0; e < MX_MAX_ELEMENTS; e++)
+    if (e < nel)
+      drift = drift || fabs(e1[e] / s1 - e0[e] / s0) > net.drift * e0[e] / s0 + 2.0 * atol * nok * net.etot / s0;
+  const int c = (xfin ? 0 : GUARD_NONFINITE) | (done ? 0 : GUARD_UNFINISHED) | (drift ? GUARD_DRIFT : 0);
+  if (c) return c;
+  // lambda of (A X A^T) lambda = e0 s1 / s0 - e1 by LDL^T; an element whose pivot vanishes is left out
+  double m[MX_MAX_ELEMENTS * MX_MAX_ELEMENTS], m0[MX_MAX_ELEMENTS], y[MX_MAX_ELEMENTS], lam[MX_MAX_ELEMENTS];
+  const double r = s1 / s0;
+#pragma unroll
+  for (int e = 0; e < MX_MAX_ELEMENTS; e++) {
+#pragma unroll
+    for (int f = 0; f < MX_MAX_ELEMENTS; f++) {
+      m[e * MX_MAX_ELEMENTS + f] = 0.0;
+      if (e < nel && f < nel && f >= e)
+        m[e * MX_MAX_ELEMENTS + f] = species_sum(ns, lane, [&](int i, double p) {
+          const double ae = __ldg(at + i * nel + e), af = __ldg(at + i * nel + f);
+          return (ae != 0.0 && af != 0.0) ? fma(ae * af, xo[i], p) : p;
+        });
+    }
+    m0[e] = m[e * MX_MAX_ELEMENTS + e];
+    y[e] = e < nel ? fma(e0[e], r, -e1[e]) : 0.0;
   }
-  for (int k = 0; k < nel; k++) {
-    if (!(m[k * nel + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
-    for (int j = k + 1; j < nel; j++) {
-      const double l = m[k * nel + j] / m[k * nel + k];
-      for (int f = j; f < nel; f++) m[j * nel + f] = fma(-l, m[k * nel + f], m[j * nel + f]);
+#pragma unroll
+  for (int k = 0; k < MX_MAX_ELEMENTS; k++) {
+    if (k >= nel || !(m[k * MX_MAX_ELEMENTS + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
+#pragma unroll
+    for (int j = k + 1; j < MX_MAX_ELEMENTS; j++) {
+      if (j >= nel) continue;
+      const double l = m[k * MX_MAX_ELEMENTS + j] / m[k * MX_MAX_ELEMENTS + k];
+#pragma unroll
+      for (int f = j; f < MX_MAX_ELEMENTS; f++)
+        if (f < nel) m[j * MX_MAX_ELEMENTS + f] = fma(-l, m[k * MX_MAX_ELEMENTS + f], m[j * MX_MAX_ELEMENTS + f]);
       y[j] = fma(-l, y[k], y[j]);
     }
   }
-  for (int k = nel - 1; k >= 0; k--) {
+#pragma unroll
+  for (int k = MX_MAX_ELEMENTS - 1; k >= 0; k--) {
     lam[k] = 0.0;
-    if (!(m[k * nel + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
+    if (k >= nel || !(m[k * MX_MAX_ELEMENTS + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
     double b = y[k];
-    for (int f = k + 1; f < nel; f++) b = fma(-m[k * nel + f], lam[f], b);
-    lam[k] = b / m[k * nel + k];
+#pragma unroll
+    for (int f = k + 1; f < MX_MAX_ELEMENTS; f++)
+      if (f < nel) b = fma(-m[k * MX_MAX_ELEMENTS + f], lam[f], b);
+    lam[k] = b / m[k * MX_MAX_ELEMENTS + k];
   }
-}
-
-// Guard bits of a stepped cell's result xo (network order) against its input x0; a passing result has its element
-// shares put back in place (check_cell).
-__device__ int check_cell(const Net& net, const double* __restrict__ x0, double* xo, int done, double nok,
-                          double atol) {
-  const int ns = net.ns, nel = net.nel;
-  double e0[MX_MAX_ELEMENTS], e1[MX_MAX_ELEMENTS], lam[MX_MAX_ELEMENTS];
-  for (int e = 0; e < nel; e++) e0[e] = e1[e] = 0.0;
-  bool xfin = true;
-  for (int i = 0; i < ns; i++) {
-    const double a = x0[i], b = xo[i];
-    xfin = xfin && isfinite(b);
-    for (int e = 0; e < nel; e++) {
-      const double at = __ldg(net.atoms + i * nel + e);
-      e0[e] = fma(at, a, e0[e]);
-      e1[e] = fma(at, b, e1[e]);
-    }
-  }
-  double s0 = 0.0, s1 = 0.0;
-  for (int e = 0; e < nel; e++) {
-    s0 += e0[e];
-    s1 += e1[e];
-  }
-  bool drift = false;
-  for (int e = 0; e < nel; e++)
-    drift = drift || fabs(e1[e] / s1 - e0[e] / s0) > net.drift * e0[e] / s0 + 2.0 * atol * nok * net.etot / s0;
-  const int c = (xfin ? 0 : GUARD_NONFINITE) | (done ? 0 : GUARD_UNFINISHED) | (drift ? GUARD_DRIFT : 0);
-  if (c) return c;
-  element_multipliers(ns, nel, xo, net.atoms, e0, e1, s1 / s0, lam);
-  double sum = 0.0;
-  for (int i = 0; i < ns; i++) {
+  double part = 0.0;
+  for (int i = lane; i < ns; i += 32) {
     double g = 1.0;
-    for (int e = 0; e < nel; e++) {
-      const double at = __ldg(net.atoms + i * nel + e);
-      if (at != 0.0) g = fma(lam[e], at, g);
+#pragma unroll
+    for (int e = 0; e < MX_MAX_ELEMENTS; e++) {
+      if (e < nel) {
+        const double a = __ldg(at + i * nel + e);
+        if (a != 0.0) g = fma(lam[e], a, g);
+      }
     }
     g = fmin(fmax(g, 1.0 - MX_GMAX), 1.0 + MX_GMAX);
-    sum = fma(xo[i], g, sum);
+    part = fma(xo[i], g, part);
     xo[i] *= g;
   }
+  const double sum = warp_sum(part);
+  __syncwarp();
   if (!(isfinite(sum) && sum > 0.0)) return GUARD_NONFINITE;
   const double is = 1.0 / sum;
-  for (int i = 0; i < ns; i++) xo[i] *= is;
+  for (int i = lane; i < ns; i += 32) xo[i] *= is;
+  __syncwarp();
   return 0;
 }
 

@@ -28,7 +28,7 @@ enum { PH_RATES, PH_RHS_JAC, PH_LU, PH_STAGE12, PH_STAGE3, PH_STAGE4, PH_CONTROL
 // The call kernel: screening, rates, Rodas3 steps, output and the guard, per cell (call.cuh:5-177, guard.cuh:114-140).
 // PROF: also sum clock64 cycles per phase into prof[PH_COUNT].
 template <int W, int R, bool PROF>
-__global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallArgs a, long long* prof) {
+__global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const CallArgs a, long long* prof) {
   extern __shared__ double smem[];
   const Cell c = cell_arrays(net, smem);
   const int tid = (int)threadIdx.x, nt = 32 * W, lane = tid & 31, warp = tid >> 5, ns = net.ns, ld = net.ld;
@@ -163,34 +163,36 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
     const double sum = c.red[3];
     for (int i = tid; i < ns; i += nt) c.Y[__ldg(net.perm + i)] = c.N[i] / sum;
     __syncthreads();
-    if (tid == 0) {
+    if (warp == 0) {
       const int done = (st == 0 && s.t >= dt * MX_CALL_END) ? 1 : 0;
-      a.h_out[cell] = s.h;
-      a.done[cell] = done;
-      a.steps[cell] = s.nok;
-      int r = 0;
-      if (st == MX_REFUSED_COLD)
-        atomicAdd(a.count + MX_COUNT_COLD, 1);
-      else if (st == MX_REFUSED_HOT)
-        atomicAdd(a.count + MX_COUNT_HOT, 1);
-      else if (st == MX_REFUSED_BAD_INPUT)
-        atomicAdd(a.count + MX_COUNT_BAD_INPUT, 1);
-      else {
-        const int g = check_cell(net, x0, c.Y, done, s.nok, a.atol);
-        if (g & GUARD_NONFINITE) atomicAdd(a.count + MX_COUNT_NONFINITE, 1);
-        if (g & GUARD_UNFINISHED) atomicAdd(a.count + MX_COUNT_UNFINISHED, 1);
-        if (g & GUARD_DRIFT) atomicAdd(a.count + MX_COUNT_DRIFT, 1);
-        if (g) {
-          r = 1;
-          a.list[atomicAdd(a.count + MX_COUNT_RECOMPUTED, 1)] = cell;
+      const int g = st == 0 ? check_cell(net, x0, c.Y, done, s.nok, a.atol, lane) : 0;
+      if (lane == 0) {
+        a.h_out[cell] = s.h;
+        a.done[cell] = done;
+        a.steps[cell] = s.nok;
+        int r = 0;
+        if (st == MX_REFUSED_COLD)
+          atomicAdd(a.count + MX_COUNT_COLD, 1);
+        else if (st == MX_REFUSED_HOT)
+          atomicAdd(a.count + MX_COUNT_HOT, 1);
+        else if (st == MX_REFUSED_BAD_INPUT)
+          atomicAdd(a.count + MX_COUNT_BAD_INPUT, 1);
+        else {
+          if (g & GUARD_NONFINITE) atomicAdd(a.count + MX_COUNT_NONFINITE, 1);
+          if (g & GUARD_UNFINISHED) atomicAdd(a.count + MX_COUNT_UNFINISHED, 1);
+          if (g & GUARD_DRIFT) atomicAdd(a.count + MX_COUNT_DRIFT, 1);
+          if (g) {
+            r = 1;
+            a.list[atomicAdd(a.count + MX_COUNT_RECOMPUTED, 1)] = cell;
+          }
         }
+        a.flag[cell] = r;
+        if (a.tries) {
+          atomicAdd(a.tries, (unsigned long long)tries);
+          atomicAdd(a.tries + 1, (unsigned long long)retries);
+        }
+        c.ints[1] = (int)(gridDim.x + atomicAdd(a.count + MX_COUNT_QUEUE, 1));
       }
-      a.flag[cell] = r;
-      if (a.tries) {
-        atomicAdd(a.tries, (unsigned long long)tries);
-        atomicAdd(a.tries + 1, (unsigned long long)retries);
-      }
-      c.ints[1] = (int)(gridDim.x + atomicAdd(a.count + MX_COUNT_QUEUE, 1));
     }
     __syncthreads();
     double* xo = a.x_out + (size_t)cell * ns;
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(32 * W) call_kernel(const Net net, const CallA
 // threshold pivoting, REC_STEPS times the tries, and up to REC_RETRIES retries with a smaller first try when only the
 // element test failed (recover.cuh:231-310).
 template <int W, int R>
-__global__ void __launch_bounds__(32 * W) recover_kernel(const Net net, const CallArgs a, int max_steps) {
+__global__ void __launch_bounds__(32 * W, 4) recover_kernel(const Net net, const CallArgs a, int max_steps) {
   const int nfl = a.count[MX_COUNT_RECOMPUTED];
   if ((int)blockIdx.x >= nfl) return;
   extern __shared__ double smem[];
@@ -293,10 +295,11 @@ __global__ void __launch_bounds__(32 * W) recover_kernel(const Net net, const Ca
       const double sum = c.red[3];
       for (int i = tid; i < ns; i += nt) c.Y[__ldg(net.perm + i)] = c.N[i] / sum;
       __syncthreads();
-      if (tid == 0) {
+      if (warp == 0) {
         const int dn = s.t >= dt * MX_CALL_END ? 1 : 0;
-        const int g = check_cell(net, x0, c.Y, dn, s.nok, a.atol);
-        if (g == GUARD_DRIFT && k < MX_REC_RETRIES) {
+        const int g = check_cell(net, x0, c.Y, dn, s.nok, a.atol, lane);
+        if (lane != 0) {
+        } else if (g == GUARD_DRIFT && k < MX_REC_RETRIES) {
           c.ints[1] = -1;  // only the element test failed: again from the inputs with a smaller first try
         } else {
           a.h_out[cell] = s.h;
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(32 * W) debug_try_kernel(const Net net, const 
 // F, Jacobian and w, LU, two-vector solve, one-vector solve, Sherman-Morrison, error, guard test. cycles[9] receives
 // the CTA-0 averages.
 template <int W, int R>
-__global__ void __launch_bounds__(32 * W) time_phases_kernel(const Net net, const double* x0, double Tc, double P,
+__global__ void __launch_bounds__(32 * W, 4) time_phases_kernel(const Net net, const double* x0, double Tc, double P,
                                                              double ha, const double* Jc, int reps,
                                                              long long* cycles) {
   extern __shared__ double smem[];
@@ -456,10 +459,11 @@ __global__ void __launch_bounds__(32 * W) time_phases_kernel(const Net net, cons
       acc[7] += u - t;
     }
     __syncthreads();
-    if (tid == 0) {
-      for (int i = 0; i < ns; i++) c.Y[__ldg(net.perm + i)] = c.N[i];
+    if (warp == 0) {
+      for (int i = lane; i < ns; i += 32) c.Y[__ldg(net.perm + i)] = c.N[i];
+      __syncwarp();
       t = clock64();
-      check_cell(net, x0, c.Y, 1, 1.0, 1e-25);
+      check_cell(net, x0, c.Y, 1, 1.0, 1e-25, lane);
       u = clock64();
       acc[8] += u - t;
     }
@@ -469,12 +473,17 @@ __global__ void __launch_bounds__(32 * W) time_phases_kernel(const Net net, cons
     for (int q = 0; q < 9; q++) cycles[q] = acc[q] / reps;
 }
 
-// The guard alone, one thread per cell (guard.cuh:114-140), on results in global memory.
-__global__ void guard_kernel(const Net net, const double* x0, double* xout, const int* done, const double* nok,
-                             const int* status, int B, double atol, int* flag, int* count, int* list) {
-  const int cell = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+// The guard alone, one warp per cell (guard.cuh:114-140), on results in global memory; 4 warps per block.
+__global__ void __launch_bounds__(128) guard_kernel(const Net net, const double* x0, double* xout, const int* done,
+                                                    const double* nok, const int* status, int B, double atol,
+                                                    int* flag, int* count, int* list) {
+  const int cell = (int)(blockIdx.x * 4 + (threadIdx.x >> 5)), lane = (int)(threadIdx.x & 31);
   if (cell >= B) return;
   const int s = status[cell];
+  const int g = s == 0 ? check_cell(net, x0 + (size_t)cell * net.ns, xout + (size_t)cell * net.ns, done[cell],
+                                    nok[cell], atol, lane)
+                       : 0;
+  if (lane != 0) return;
   int r = 0;
   if (s == MX_REFUSED_COLD)
     atomicAdd(count + MX_COUNT_COLD, 1);
@@ -483,8 +492,6 @@ __global__ void guard_kernel(const Net net, const double* x0, double* xout, cons
   else if (s == MX_REFUSED_BAD_INPUT)
     atomicAdd(count + MX_COUNT_BAD_INPUT, 1);
   else {
-    const int g = check_cell(net, x0 + (size_t)cell * net.ns, xout + (size_t)cell * net.ns, done[cell], nok[cell],
-                             atol);
     if (g & GUARD_NONFINITE) atomicAdd(count + MX_COUNT_NONFINITE, 1);
     if (g & GUARD_UNFINISHED) atomicAdd(count + MX_COUNT_UNFINISHED, 1);
     if (g & GUARD_DRIFT) atomicAdd(count + MX_COUNT_DRIFT, 1);
@@ -792,7 +799,7 @@ extern "C" int mx_guard(mx_solver* s, const double* x, double* x_out, const int3
   if (rc) return rc;
   cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
   if (e == cudaSuccess && B > 0) {
-    guard_kernel<<<(int)((B + 127) / 128), 128, 0, st>>>(s->net, x, x_out, done, steps, status, (int)B, atol, flag,
+    guard_kernel<<<(int)((B + 3) / 4), 128, 0, st>>>(s->net, x, x_out, done, steps, status, (int)B, atol, flag,
                                                           count, s->list);
     e = cudaGetLastError();
   }
