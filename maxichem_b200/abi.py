@@ -40,6 +40,15 @@ class MxNetwork(ctypes.Structure):
         ("jac_entry", ctypes.c_void_p),
         ("jac_term", ctypes.c_void_p),
         ("fill", ctypes.c_void_p),
+        ("stream_threads", ctypes.c_int32 * 2),
+        ("sv_rounds", ctypes.c_int32 * 2),
+        ("sv_nrows", ctypes.c_int32 * 2),
+        ("jac_rounds", ctypes.c_int32 * 2),
+        ("jac_nents", ctypes.c_int32 * 2),
+        ("sv_stream", ctypes.c_void_p * 2),
+        ("sv_rows", ctypes.c_void_p * 2),
+        ("jac_stream", ctypes.c_void_p * 2),
+        ("jac_dst", ctypes.c_void_p * 2),
     ]
 
 
@@ -63,6 +72,17 @@ class NetworkStruct:
             jac_ptr=ptr(tab.jac_ptr, np.int32), jac_entry=ptr(tab.jac_entry, np.uint32),
             jac_term=ptr(tab.jac_term, np.uint32), fill=ptr(tab.fill, np.uint8),
         )  # fmt: skip
+        for g, threads in enumerate((128, 96)):
+            st = tab.streams.get(threads)
+            if st is None:
+                continue
+            self.struct.stream_threads[g] = threads
+            self.struct.sv_rounds[g], self.struct.sv_nrows[g] = st["sv"].shape[0], st["sv_rows"].shape[0]
+            self.struct.jac_rounds[g], self.struct.jac_nents[g] = st["jt"].shape[0], st["jac_dst"].shape[0]
+            self.struct.sv_stream[g] = ptr(st["sv"], np.uint16)
+            self.struct.sv_rows[g] = ptr(st["sv_rows"], np.uint16)
+            self.struct.jac_stream[g] = ptr(st["jt"], np.uint32)
+            self.struct.jac_dst[g] = ptr(st["jac_dst"], np.uint16)
 
     def ref(self) -> Any:
         return ctypes.byref(self.struct)

@@ -36,6 +36,12 @@ struct Net {
   const uint32_t* jac_entry;
   const uint32_t* jac_term;
   double etot, drift;
+  // per-thread streams of the S v and Jacobian sums for the CTA (group 0) and its last 96 threads (group 1)
+  int st_threads[2], sv_rounds[2], sv_nrows[2], jac_rounds[2], jac_nents[2];
+  const uint16_t* sv[2];
+  const uint16_t* sv_rows[2];
+  const uint32_t* jt[2];
+  const uint16_t* jd[2];
   // shared-memory layout
   int ld, oA, oK, oV, on, oN, oY, oF, oU, oK1, oK2, oK3, oK4, oD, oRed, oInts, doubles;
 };
@@ -172,6 +178,7 @@ __device__ __forceinline__ void cell_rates(const Net& net, const Cell& c, double
     c.kf[r] = kf;
     c.kr[r] = kr;
   }
+  if (tid == 0) c.kf[2 * net.nr] = 0.0;  // the zero rate of the Jacobian stream's padding
   __syncthreads();
 }
 
@@ -186,7 +193,10 @@ __device__ __forceinline__ double rhs(const Net& net, const Cell& c, const doubl
   const int lane = gtid & 31, ns = net.ns;
   const double ntot = lane_sum(Y, ns, lane), xf = nd / ntot, ixf = ntot / nd;
   for (int i = gtid; i < ns; i += gnt) c.n[i] = Y[i] * xf;
-  if (gtid == 0) c.n[ns] = 1.0;
+  if (gtid == 0) {
+    c.n[ns] = 1.0;
+    c.v[net.nr] = 0.0;
+  }
   group_sync(bar, gnt);
   const double* n = c.n;
   for (int r = gtid; r < net.nr; r += gnt) {
@@ -196,15 +206,24 @@ __device__ __forceinline__ double rhs(const Net& net, const Cell& c, const doubl
     c.v[r] = a - b;
   }
   group_sync(bar, gnt);
-  for (int i = gtid; i < ns; i += gnt) {
-    double s = 0.0;
-    const int t1 = __ldg(net.sv_ptr + i + 1);
-    for (int t = __ldg(net.sv_ptr + i); t < t1; t++) {
-      const unsigned w = __ldg(net.sv_term + t);
-      s = fma(code_coefficient(w >> 16), c.v[w & 0xffffu], s);
+  // S v: each thread its rows (ascending reactions) from its coalesced word stream; v[nr] = 0 pads the streams
+  const int g = gnt == net.st_threads[0] ? 0 : 1;
+  const uint16_t* __restrict__ sw = net.sv[g] + gtid;
+  const uint16_t* __restrict__ sr = net.sv_rows[g] + gtid;
+  double s = 0.0;
+  int row = 0;
+  const int rounds = net.sv_rounds[g];
+#pragma unroll 4
+  for (int q = 0; q < rounds; q++) {
+    const unsigned w = __ldg(sw + q * gnt);
+    s = fma(code_coefficient(w >> 11), c.v[w & 0x7ffu], s);
+    if (w & 0x2000u) {
+      const int i = __ldg(sr + row * gnt);
+      c.F[i] = s * ixf;
+      if (u0) c.U[i] = s / nd;
+      s = 0.0;
+      row++;
     }
-    c.F[i] = s * ixf;
-    if (u0) c.U[i] = s / nd;
   }
   group_sync(bar, gnt);
   return ntot;
@@ -220,16 +239,23 @@ __device__ __forceinline__ void jacobian_w(const Net& net, const Cell& c, double
   const int ns = net.ns, ld = net.ld;
   for (int i = tid; i < ns * ld; i += nt) c.A[i] = 0.0;
   __syncthreads();
-  for (int e = tid; e < net.n_entries; e += nt) {
+  {  // each thread its entries from its coalesced word stream; the padding words use the zero rate kf[2 nr]
+    const uint32_t* __restrict__ jw = net.jt[0] + tid;
+    const uint16_t* __restrict__ jd = net.jd[0] + tid;
+    const int rounds = net.jac_rounds[0];
     double acc = 0.0;
-    const int t1 = __ldg(net.jac_ptr + e + 1);
-    for (int t = __ldg(net.jac_ptr + e); t < t1; t++) {
-      const unsigned w = __ldg(net.jac_term + t);
+    int e = 0;
+#pragma unroll 4
+    for (int q = 0; q < rounds; q++) {
+      const unsigned w = __ldg(jw + q * nt);
       const double pr = c.kf[w & 0xfffu] * c.n[(w >> 16) & 255u] * c.n[w >> 24];
       acc = fma(code_coefficient(w >> 12), pr, acc);
+      if (w & 0x4000u) {
+        c.A[__ldg(jd + e * nt)] = -acc;
+        acc = 0.0;
+        e++;
+      }
     }
-    const unsigned pq = __ldg(net.jac_entry + e);
-    c.A[(int)(pq >> 16) * ld + (int)(pq & 0xffffu)] = -acc;
   }
   __syncthreads();
   for (int i = tid; i < ns; i += nt) {
@@ -299,26 +325,40 @@ __device__ __forceinline__ void lu_factor(const Net& net, double* A, double* din
   const int ns = net.ns, ld = net.ld;
   for (int kb = 0; kb < ns; kb += PANEL) {
     const int ke = min(kb + PANEL, ns), nb = ke - kb;
-    if (tid == 0) dinv[kb] = 1.0 / A[kb * ld + kb];
+    if (tid == 0) dinv[kb] = __drcp_rn(A[kb * ld + kb]);  // 1 / x, correctly rounded: the bits of 1.0 / x
     __syncthreads();
     for (int k = kb; k < ke; k++) {  // the panel: columns kb..ke-1
       const double d = dinv[k];
+      double piv[PANEL];
+#pragma unroll
+      for (int jj = 1; jj < PANEL; jj++) piv[jj] = k + jj < ke ? A[k * ld + k + jj] : 0.0;
       for (int i = k + 1 + tid; i < ns; i += NT) {
         double* ai = A + i * ld;
         const double l = ai[k] * d;
         ai[k] = l;
-        for (int j = k + 1; j < ke; j++) ai[j] = fma(-l, A[k * ld + j], ai[j]);
-        if (i == k + 1 && i < ke) dinv[i] = 1.0 / ai[i];  // the next pivot, final now
+#pragma unroll
+        for (int jj = 1; jj < PANEL; jj++)
+          if (k + jj < ke) ai[k + jj] = fma(-l, piv[jj], ai[k + jj]);
+        if (i == k + 1 && i < ke) dinv[i] = __drcp_rn(ai[i]);  // the next pivot, final now
       }
       __syncthreads();
     }
     if (ke == ns) break;
     // the block's pivot rows beyond the panel: row kb + s takes pivots kb .. kb + s - 1
     for (int j = ke + tid; j < ns; j += NT) {
-      for (int s = 1; s < nb; s++) {
-        double a = A[(kb + s) * ld + j];
-        for (int t = 0; t < s; t++) a = fma(-A[(kb + s) * ld + kb + t], A[(kb + t) * ld + j], a);
-        A[(kb + s) * ld + j] = a;
+      double row[PANEL];
+#pragma unroll
+      for (int s = 0; s < PANEL; s++) row[s] = s < nb ? A[(kb + s) * ld + j] : 0.0;
+#pragma unroll
+      for (int s = 1; s < PANEL; s++) {
+        if (s < nb) {
+          double a = row[s];
+#pragma unroll
+          for (int t = 0; t < PANEL; t++)
+            if (t < s) a = fma(-A[(kb + s) * ld + kb + t], row[t], a);
+          row[s] = a;
+          A[(kb + s) * ld + j] = a;
+        }
       }
     }
     __syncthreads();
@@ -338,13 +378,14 @@ __device__ __forceinline__ double pick(const double (&a)[R], int idx) {
 }
 
 // y <- M0^-1 y on one warp for NV vectors (1 or 2) with the factors of lu_factor: lane l holds rows l + 32 p.
-// Forward unit L in ascending k, U in descending k with x_k = a_k / U_kk (msolve, common.cuh:504-522), four pivots
-// per round: the four pivot rows' current values are broadcast at once and every lane finishes those four itself
-// (a 4 x 4 triangle), then updates its own rows with the four in order. Each entry receives the same fma's in the
-// same order as the one-pivot sweep, so the bits are those of the one-pivot sweep.
+// Forward unit L in ascending k, U in descending k with x_k = a_k / U_kk (msolve, common.cuh:504-522). Pivots are
+// taken 32 at a time, so the pivot's value comes from a register chosen at compile time (c) and one shuffle; the next
+// column of L or U is loaded while the current pivot is applied. A lane whose row takes no update from pivot k uses
+// the multiplier 0, and fma(-0, y, a) = a for finite y. Each entry receives the one-pivot sweep's fma's in its order.
 template <int R, int NV>
-__device__ __forceinline__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1, int lane) {
-  const int ns = net.ns, ld = net.ld;
+__device__ __forceinline__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1,
+                                         int lane) {
+  const int ns = net.ns, ld = net.ld, last = ns - 1;
   double a[NV][R], d[R];
 #pragma unroll
   for (int p = 0; p < R; p++) {
@@ -353,97 +394,53 @@ __device__ __forceinline__ void lu_solve(const Net& net, const double* A, const 
     a[0][p] = i < ns ? y0[i] : 0.0;
     if (NV == 2) a[NV - 1][p] = i < ns ? y1[i] : 0.0;
   }
-  // forward: pivots kb .. kb + q - 1 (the last row takes no pivot of its own)
-  for (int kb = 0; kb < ns - 1; kb += 4) {
-    const int q = min(4, ns - 1 - kb);
-    double yv[NV][4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int k = min(kb + j, ns - 1);
+  for (int c = 0; c < R; c++) {  // forward: pivots 32c .. 32c + 31
+    const int k0 = 32 * c, k1 = min(k0 + 32, last);
+    if (k0 >= k1) break;
+    double m[R];
 #pragma unroll
-      for (int v = 0; v < NV; v++) yv[v][j] = __shfl_sync(FULL, pick<R>(a[v], k >> 5), k & 31);
-    }
-    double lt[6];  // L[kb+1][kb], L[kb+2][kb], L[kb+2][kb+1], L[kb+3][kb], L[kb+3][kb+1], L[kb+3][kb+2]
-    lt[0] = q > 1 ? A[(kb + 1) * ld + kb] : 0.0;
-    lt[1] = q > 2 ? A[(kb + 2) * ld + kb] : 0.0;
-    lt[2] = q > 2 ? A[(kb + 2) * ld + kb + 1] : 0.0;
-    lt[3] = q > 3 ? A[(kb + 3) * ld + kb] : 0.0;
-    lt[4] = q > 3 ? A[(kb + 3) * ld + kb + 1] : 0.0;
-    lt[5] = q > 3 ? A[(kb + 3) * ld + kb + 2] : 0.0;
+    for (int p = c; p < R; p++) m[p] = A[min(lane + 32 * p, last) * ld + k0];
+#pragma unroll 4
+    for (int k = k0; k < k1; k++) {
+      double yk[NV];
 #pragma unroll
-    for (int v = 0; v < NV; v++) {
-      yv[v][1] = fma(-lt[0], yv[v][0], yv[v][1]);
-      yv[v][2] = fma(-lt[2], yv[v][1], fma(-lt[1], yv[v][0], yv[v][2]));
-      yv[v][3] = fma(-lt[5], yv[v][2], fma(-lt[4], yv[v][1], fma(-lt[3], yv[v][0], yv[v][3])));
-    }
+      for (int v = 0; v < NV; v++) yk[v] = __shfl_sync(FULL, a[v][c], k & 31);
+      double mn[R];
 #pragma unroll
-    for (int p = 0; p < R; p++) {
-      if (32 * p + 31 <= kb) continue;  // the whole block of rows is final (warp-uniform)
-      const int i = lane + 32 * p;
-      const bool upd = i >= kb + q && i < ns;
-      const double* ai = A + min(i, ns - 1) * ld + kb;  // a valid row whether or not this one is updated
-      double m[4];
+      for (int p = c; p < R; p++) mn[p] = A[min(lane + 32 * p, last) * ld + min(k + 1, last)];
 #pragma unroll
-      for (int j = 0; j < 4; j++) m[j] = j < q ? ai[j] : 0.0;
+      for (int p = c; p < R; p++) {
+        const bool act = (p > c ? true : lane > k - k0) && lane + 32 * p < ns;
+        const double mm = act ? m[p] : 0.0;
 #pragma unroll
-      for (int v = 0; v < NV; v++) {
-        double t = a[v][p];
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (j < q) t = fma(-m[j], yv[v][j], t);
-        // rows kb+1 .. kb+q-1 take the values finished above; rows at or before kb keep theirs
-        const double fin = i == kb + 1 ? yv[v][1] : (i == kb + 2 ? yv[v][2] : (i == kb + 3 ? yv[v][3] : a[v][p]));
-        a[v][p] = upd ? t : fin;
+        for (int v = 0; v < NV; v++) a[v][p] = fma(-mm, yk[v], a[v][p]);
+        m[p] = mn[p];
       }
     }
   }
-  // backward: pivots hi, hi - 1, .., lo (descending), x_k = a_k d_k; rows below lo take them in that order
-  for (int hi = ns - 1; hi > 0; hi -= 4) {
-    const int lo = max(hi - 3, 1), q = hi - lo + 1;
-    double av[NV][4], dv[4], ut[6];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int k = max(hi - j, 0);
+  for (int c = R - 1; c >= 0; c--) {  // backward: pivots 32c + 31 .. 32c (down to 1)
+    const int k0 = 32 * c, khi = min(k0 + 31, last), klo = max(k0, 1);
+    if (khi < klo) continue;
+    double m[R];
 #pragma unroll
-      for (int v = 0; v < NV; v++) av[v][j] = __shfl_sync(FULL, pick<R>(a[v], k >> 5), k & 31);
-      dv[j] = dinv[k];
-    }
-    // U[hi-1][hi], U[hi-2][hi], U[hi-2][hi-1], U[hi-3][hi], U[hi-3][hi-1], U[hi-3][hi-2]
-    ut[0] = q > 1 ? A[(hi - 1) * ld + hi] : 0.0;
-    ut[1] = q > 2 ? A[(hi - 2) * ld + hi] : 0.0;
-    ut[2] = q > 2 ? A[(hi - 2) * ld + hi - 1] : 0.0;
-    ut[3] = q > 3 ? A[(hi - 3) * ld + hi] : 0.0;
-    ut[4] = q > 3 ? A[(hi - 3) * ld + hi - 1] : 0.0;
-    ut[5] = q > 3 ? A[(hi - 3) * ld + hi - 2] : 0.0;
-    double z[NV][4];
+    for (int p = 0; p <= c; p++) m[p] = A[min(lane + 32 * p, last) * ld + khi];
+#pragma unroll 4
+    for (int k = khi; k >= klo; k--) {
+      double z[NV];
 #pragma unroll
-    for (int v = 0; v < NV; v++) {
-      z[v][0] = av[v][0] * dv[0];
-      av[v][1] = fma(-ut[0], z[v][0], av[v][1]);
-      z[v][1] = av[v][1] * dv[1];
-      av[v][2] = fma(-ut[2], z[v][1], fma(-ut[1], z[v][0], av[v][2]));
-      z[v][2] = av[v][2] * dv[2];
-      av[v][3] = fma(-ut[5], z[v][2], fma(-ut[4], z[v][1], fma(-ut[3], z[v][0], av[v][3])));
-      z[v][3] = av[v][3] * dv[3];
-    }
+      for (int v = 0; v < NV; v++) z[v] = __shfl_sync(FULL, a[v][c] * d[c], k & 31);
+      double mn[R];
 #pragma unroll
-    for (int p = 0; p < R; p++) {
-      if (32 * p >= hi) continue;  // every row of the block is at or after hi (warp-uniform)
-      const int i = lane + 32 * p;
-      const bool upd = i < lo;
-      const double* ai = A + min(i, ns - 1) * ld;
-      double m[4];
+      for (int p = 0; p <= c; p++) mn[p] = A[min(lane + 32 * p, last) * ld + max(k - 1, 0)];
 #pragma unroll
-      for (int j = 0; j < 4; j++) m[j] = j < q ? ai[hi - j] : 0.0;
+      for (int p = 0; p <= c; p++) {
+        const bool act = p < c ? true : lane < k - k0;
+        const double mm = act ? m[p] : 0.0;
 #pragma unroll
-      for (int v = 0; v < NV; v++) {
-        double t = a[v][p];
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (j < q) t = fma(-m[j], z[v][j], t);
-        // rows lo .. hi-1 take the values finished above; rows from hi on keep theirs
-        const double fin = i == hi - 1 ? av[v][1] : (i == hi - 2 ? av[v][2] : (i == hi - 3 ? av[v][3] : a[v][p]));
-        a[v][p] = upd ? t : fin;
+        for (int v = 0; v < NV; v++) a[v][p] = fma(-mm, z[v], a[v][p]);
+        m[p] = mn[p];
       }
     }
   }
@@ -610,18 +607,17 @@ __device__ __forceinline__ double species_sum(int ns, int lane, F f) {
 // Guard bits of a stepped cell's result xo (network order, shared memory) against its input x0; a passing result
 // has its element shares put back in place (check_cell): x' = x (1 + sum_e lambda_e a_ie), clamped, renormalised.
 // Every lane of the warp returns the bits.
-__device__ __noinline__ int check_cell(const Net& net, const double* __restrict__ x0, double* xo, int done, double nok,
-                                       double atol, int lane) {
+__device__ __noinline__ int check_cell(const Net& net, const double* x0, double* xo, int done, double nok,
+                                       double atol, int lane, const double* at) {
   const int ns = net.ns, nel = net.nel;
-  const double* __restrict__ at = net.atoms;
   double e0[MX_MAX_ELEMENTS], e1[MX_MAX_ELEMENTS];
   double s0 = 0.0, s1 = 0.0;
 #pragma unroll
   for (int e = 0; e < MX_MAX_ELEMENTS; e++) {
     e0[e] = e1[e] = 0.0;
     if (e < nel) {
-      e0[e] = species_sum(ns, lane, [&](int i, double p) { return fma(__ldg(at + i * nel + e), x0[i], p); });
-      e1[e] = species_sum(ns, lane, [&](int i, double p) { return fma(__ldg(at + i * nel + e), xo[i], p); });
+      e0[e] = species_sum(ns, lane, [&](int i, double p) { return fma(at[i * nel + e], x0[i], p); });
+      e1[e] = species_sum(ns, lane, [&](int i, double p) { return fma(at[i * nel + e], xo[i], p); });
       s0 += e0[e];
       s1 += e1[e];
     }
@@ -646,7 +642,7 @@ __device__ __noinline__ int check_cell(const Net& net, const double* __restrict_
       m[e * MX_MAX_ELEMENTS + f] = 0.0;
       if (e < nel && f < nel && f >= e)
         m[e * MX_MAX_ELEMENTS + f] = species_sum(ns, lane, [&](int i, double p) {
-          const double ae = __ldg(at + i * nel + e), af = __ldg(at + i * nel + f);
+          const double ae = at[i * nel + e], af = at[i * nel + f];
           return (ae != 0.0 && af != 0.0) ? fma(ae * af, xo[i], p) : p;
         });
     }
@@ -682,7 +678,7 @@ __device__ __noinline__ int check_cell(const Net& net, const double* __restrict_
 #pragma unroll
     for (int e = 0; e < MX_MAX_ELEMENTS; e++) {
       if (e < nel) {
-        const double a = __ldg(at + i * nel + e);
+        const double a = at[i * nel + e];
         if (a != 0.0) g = fma(lam[e], a, g);
       }
     }

@@ -22,6 +22,18 @@ namespace {
 
 constexpr int WARPS = 4;  // warps per cell
 
+// The guard's inputs into the matrix's space, free once the steps are done: atoms [ns][nel] and the cell's input row,
+// so the guard's species sums read shared memory. Falls back to global memory when they do not fit.
+__device__ __forceinline__ void stage_guard_inputs(const Net& net, const Cell& c, const double* x0, int tid, int nt,
+                                                   const double** at, const double** xin) {
+  const int ns = net.ns, na = ns * net.nel;
+  if (na + ns > ns * net.ld) return;
+  for (int e = tid; e < na; e += nt) c.A[e] = __ldg(net.atoms + e);
+  for (int i = tid; i < ns; i += nt) c.A[na + i] = x0[i];
+  *at = c.A;
+  *xin = c.A + na;
+}
+
 // Phases of a try that the profiling variant of the call kernel times (clock64 on thread 0, summed over cells).
 enum { PH_RATES, PH_RHS_JAC, PH_LU, PH_STAGE12, PH_STAGE3, PH_STAGE4, PH_CONTROL, PH_OUTPUT, PH_COUNT };
 
@@ -162,10 +174,12 @@ __global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const Ca
     __syncthreads();
     const double sum = c.red[3];
     for (int i = tid; i < ns; i += nt) c.Y[__ldg(net.perm + i)] = c.N[i] / sum;
+    const double *at = net.atoms, *xin = x0;
+    stage_guard_inputs(net, c, x0, tid, nt, &at, &xin);
     __syncthreads();
     if (warp == 0) {
       const int done = (st == 0 && s.t >= dt * MX_CALL_END) ? 1 : 0;
-      const int g = st == 0 ? check_cell(net, x0, c.Y, done, s.nok, a.atol, lane) : 0;
+      const int g = st == 0 ? check_cell(net, xin, c.Y, done, s.nok, a.atol, lane, at) : 0;
       if (lane == 0) {
         a.h_out[cell] = s.h;
         a.done[cell] = done;
@@ -294,10 +308,12 @@ __global__ void __launch_bounds__(32 * W, 4) recover_kernel(const Net net, const
       __syncthreads();
       const double sum = c.red[3];
       for (int i = tid; i < ns; i += nt) c.Y[__ldg(net.perm + i)] = c.N[i] / sum;
+      const double *at = net.atoms, *xin = x0;
+      stage_guard_inputs(net, c, x0, tid, nt, &at, &xin);
       __syncthreads();
       if (warp == 0) {
         const int dn = s.t >= dt * MX_CALL_END ? 1 : 0;
-        const int g = check_cell(net, x0, c.Y, dn, s.nok, a.atol, lane);
+        const int g = check_cell(net, xin, c.Y, dn, s.nok, a.atol, lane, at);
         if (lane != 0) {
         } else if (g == GUARD_DRIFT && k < MX_REC_RETRIES) {
           c.ints[1] = -1;  // only the element test failed: again from the inputs with a smaller first try
@@ -463,7 +479,7 @@ __global__ void __launch_bounds__(32 * W, 4) time_phases_kernel(const Net net, c
       for (int i = lane; i < ns; i += 32) c.Y[__ldg(net.perm + i)] = c.N[i];
       __syncwarp();
       t = clock64();
-      check_cell(net, x0, c.Y, 1, 1.0, 1e-25, lane);
+      check_cell(net, x0, c.Y, 1, 1.0, 1e-25, lane, net.atoms);
       u = clock64();
       acc[8] += u - t;
     }
@@ -481,7 +497,7 @@ __global__ void __launch_bounds__(128) guard_kernel(const Net net, const double*
   if (cell >= B) return;
   const int s = status[cell];
   const int g = s == 0 ? check_cell(net, x0 + (size_t)cell * net.ns, xout + (size_t)cell * net.ns, done[cell],
-                                    nok[cell], atol, lane)
+                                    nok[cell], atol, lane, net.atoms)
                        : 0;
   if (lane != 0) return;
   int r = 0;
@@ -648,7 +664,7 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   };
   net.oA = take(ns * net.ld);
   net.oK = take(2 * nr + 2);
-  net.oV = take(std::max(nr, ns + 1));
+  net.oV = take(std::max(nr + 1, ns + 1));
   net.on = take(ns + 1);
   net.oN = take(ns);
   net.oY = take(ns);
@@ -694,6 +710,12 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
     rx8[r] = w;
   }
   const int nsv = n->sv_ptr[ns], njt = n->jac_ptr[n->n_entries];
+  if (n->stream_threads[0] != 32 * WARPS || n->stream_threads[1] != 32 * (WARPS - 1)) {
+    set_error(err, errlen, "mx_create: the tables' thread streams are for %d and %d threads; the kernels use %d and %d",
+              n->stream_threads[0], n->stream_threads[1], 32 * WARPS, 32 * (WARPS - 1));
+    delete s;
+    return MX_ERR_NETWORK;
+  }
   if (e == cudaSuccess) e = upload(s, n->perm, ns, &net.perm);
   if (e == cudaSuccess) e = upload(s, rx8.data(), nr, &net.rx8);
   if (e == cudaSuccess) e = upload(s, n->rc, (size_t)nr * 14, &net.rc);
@@ -705,6 +727,18 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   if (e == cudaSuccess) e = upload(s, n->jac_ptr, n->n_entries + 1, &net.jac_ptr);
   if (e == cudaSuccess) e = upload(s, n->jac_entry, n->n_entries, &net.jac_entry);
   if (e == cudaSuccess) e = upload(s, n->jac_term, njt, &net.jac_term);
+  for (int g = 0; g < 2 && e == cudaSuccess; g++) {
+    const int t = n->stream_threads[g];
+    net.st_threads[g] = t;
+    net.sv_rounds[g] = n->sv_rounds[g];
+    net.sv_nrows[g] = n->sv_nrows[g];
+    net.jac_rounds[g] = n->jac_rounds[g];
+    net.jac_nents[g] = n->jac_nents[g];
+    e = upload(s, n->sv_stream[g], (size_t)n->sv_rounds[g] * t, &net.sv[g]);
+    if (e == cudaSuccess) e = upload(s, n->sv_rows[g], (size_t)n->sv_nrows[g] * t, &net.sv_rows[g]);
+    if (e == cudaSuccess) e = upload(s, n->jac_stream[g], (size_t)n->jac_rounds[g] * t, &net.jt[g]);
+    if (e == cudaSuccess) e = upload(s, n->jac_dst[g], (size_t)n->jac_nents[g] * t, &net.jd[g]);
+  }
   if (e != cudaSuccess) {
     set_error(err, errlen, "mx_create: %s", cudaGetErrorString(e));
     release(s);

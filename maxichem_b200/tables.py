@@ -130,6 +130,7 @@ class Tables:
     has_troe: bool
     has_eff: bool
     flops: dict[str, float] = field(default_factory=dict)
+    streams: dict[int, dict[str, np.ndarray]] = field(default_factory=dict)  # per-thread term streams by group size
     species: list[str] = field(default_factory=list)
     elements: list[str] = field(default_factory=list)
     photo: bool = False
@@ -234,7 +235,69 @@ def build(net: VulcanNetwork, photo: bool) -> Tables:
         species=list(net.species), elements=list(net.elements), photo=photo,
     )  # fmt: skip
     tab.flops = work_counts(tab)
+    for threads in STREAM_GROUPS:
+        tab.streams[threads] = thread_streams(tab, threads)
     return tab
+
+
+STREAM_GROUPS = (128, 96)  # the call kernel's CTA, and its warps 1-3 (which evaluate F(Y3) during stage 2)
+SV_END = 1 << 13
+J_END = 1 << 14
+
+
+def _balance(sizes: list[int], threads: int) -> list[list[int]]:
+    """Items over threads, longest first onto the least-loaded thread (ties to the lower thread)."""
+    lanes: list[list[int]] = [[] for _ in range(threads)]
+    load = np.zeros(threads, np.int64)
+    for item in sorted(range(len(sizes)), key=lambda q: (-sizes[q], q)):
+        t = int(np.argmin(load))
+        lanes[t].append(item)
+        load[t] += sizes[item]
+    return lanes
+
+
+def thread_streams(tab: Tables, threads: int) -> dict[str, np.ndarray]:
+    """Each thread's S v rows and Jacobian entries as coalesced word streams (word q of thread t at q * threads + t).
+
+    S v: a thread sums its rows one after the other, each in ascending reaction order; a word is the reaction
+    (11 bits; nr is the zero padding), the coefficient code << 11 and SV_END on a row's last term; sv_rows lists its
+    rows. Jacobian: a thread forms its entries one after the other, each in its term order; a word is the rate index
+    | code << 12 | J_END | a << 16 | b << 24, padding rate 2 nr (a zero) with a = b = ns; jac_dst lists the dense index
+    p ld + q of its entries, ld = ns | 1. The order of every sum is the plain one, so the bits do not change.
+    """
+    ns, nr = tab.ns, tab.nr
+    ld = ns | 1
+    rows = [list(range(tab.sv_ptr[i], tab.sv_ptr[i + 1])) for i in range(ns)]
+    by_thread = _balance([len(r) for r in rows], threads)
+    rounds = max(1, max(sum(len(rows[i]) for i in its) for its in by_thread))
+    nrow = max(1, max(len(its) for its in by_thread))
+    sv = np.full((rounds, threads), nr, np.uint16)
+    sv_rows = np.zeros((nrow, threads), np.uint16)
+    for t, its in enumerate(by_thread):
+        q = 0
+        for e, i in enumerate(its):
+            sv_rows[e, t] = i
+            for n, term in enumerate(rows[i]):
+                w = int(tab.sv_term[term])
+                sv[q, t] = (w & 0xFFFF) | ((w >> 16) & 3) << 11 | (SV_END if n == len(rows[i]) - 1 else 0)
+                q += 1
+    terms = [list(range(tab.jac_ptr[e], tab.jac_ptr[e + 1])) for e in range(len(tab.jac_entry))]
+    by_thread = _balance([len(t) for t in terms], threads)
+    jrounds = max(1, max(sum(len(terms[e]) for e in its) for its in by_thread))
+    jn = max(1, max(len(its) for its in by_thread))
+    pad = (2 * nr) | ns << 16 | ns << 24
+    jt = np.full((jrounds, threads), pad, np.uint32)
+    jd = np.zeros((jn, threads), np.uint16)
+    for t, its in enumerate(by_thread):
+        q = 0
+        for n, e in enumerate(its):
+            pq = int(tab.jac_entry[e])
+            jd[n, t] = (pq >> 16) * ld + (pq & 0xFFFF)
+            for m, term in enumerate(terms[e]):
+                w = int(tab.jac_term[term])
+                jt[q, t] = (w & 0x3FFF) | (J_END if m == len(terms[e]) - 1 else 0) | (w & 0xFFFF0000)
+                q += 1
+    return {"sv": sv, "sv_rows": sv_rows, "jt": jt, "jac_dst": jd}
 
 
 def work_counts(tab: Tables) -> dict[str, float]:
