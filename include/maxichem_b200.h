@@ -95,12 +95,16 @@ typedef struct mx_network {
   const uint32_t* jac_entry;     /* row << 16 | column */
   const uint32_t* jac_term;      /* rate index | code << 12 | a << 16 | b << 24 */
   const uint8_t* fill;           /* [ns][ns] pattern of L + U (the oracle's sparse factorisation) */
+  /* S v rows in pieces of sv_piece terms (the last may be shorter; a row with no terms has one empty piece): row i
+   * is the sum, in order, of pieces sv_row_ptr[i] .. sv_row_ptr[i + 1] - 1, each summed in ascending reaction order. */
+  int32_t sv_piece, n_pieces;
+  const int32_t* sv_row_ptr;     /* [ns + 1] */
   /* Per-thread streams of the same sums for the call kernel's thread groups (maxichem_b200/tables.py
    * thread_streams): [0] the CTA of 128 threads, [1] its last 96 threads. Word q of thread t at q * threads + t. */
   int32_t stream_threads[2];
   int32_t sv_rounds[2], sv_nrows[2], jac_rounds[2], jac_nents[2];
   const uint16_t* sv_stream[2];  /* reaction | code << 11 | end << 13 (padding: nr) */
-  const uint16_t* sv_rows[2];    /* the rows each thread sums */
+  const uint16_t* sv_rows[2];    /* the pieces each thread sums */
   const uint32_t* jac_stream[2]; /* rate | code << 12 | end << 14 | a << 16 | b << 24 (padding: rate 2 nr) */
   const uint16_t* jac_dst[2];    /* dense index p ld + q of each thread's entries, ld = ns | 1 */
 } mx_network;

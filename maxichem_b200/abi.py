@@ -9,6 +9,7 @@ from typing import Any
 
 import numpy as np
 
+from . import tables
 from .tables import Tables
 
 PACKAGE = Path(__file__).resolve().parent
@@ -40,6 +41,9 @@ class MxNetwork(ctypes.Structure):
         ("jac_entry", ctypes.c_void_p),
         ("jac_term", ctypes.c_void_p),
         ("fill", ctypes.c_void_p),
+        ("sv_piece", ctypes.c_int32),
+        ("n_pieces", ctypes.c_int32),
+        ("sv_row_ptr", ctypes.c_void_p),
         ("stream_threads", ctypes.c_int32 * 2),
         ("sv_rounds", ctypes.c_int32 * 2),
         ("sv_nrows", ctypes.c_int32 * 2),
@@ -72,6 +76,9 @@ class NetworkStruct:
             jac_ptr=ptr(tab.jac_ptr, np.int32), jac_entry=ptr(tab.jac_entry, np.uint32),
             jac_term=ptr(tab.jac_term, np.uint32), fill=ptr(tab.fill, np.uint8),
         )  # fmt: skip
+        piece, row_ptr = tables.sv_row_pieces(tab)
+        self.struct.sv_piece, self.struct.n_pieces = piece, int(row_ptr[-1])
+        self.struct.sv_row_ptr = ptr(row_ptr, np.int32)
         for g, threads in enumerate((128, 96)):
             st = tab.streams.get(threads)
             if st is None:

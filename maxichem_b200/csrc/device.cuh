@@ -37,13 +37,14 @@ struct Net {
   const uint32_t* jac_term;
   double etot, drift;
   // per-thread streams of the S v and Jacobian sums for the CTA (group 0) and its last 96 threads (group 1)
-  int st_threads[2], sv_rounds[2], sv_nrows[2], jac_rounds[2], jac_nents[2];
+  int st_threads[2], sv_rounds[2], sv_nrows[2], jac_rounds[2], jac_nents[2], n_pieces;
+  const int* sv_row_ptr;
   const uint16_t* sv[2];
   const uint16_t* sv_rows[2];
   const uint32_t* jt[2];
   const uint16_t* jd[2];
   // shared-memory layout
-  int ld, oA, oK, oV, on, oN, oY, oF, oU, oK1, oK2, oK3, oK4, oD, oRed, oInts, doubles;
+  int ld, oA, oK, oV, on, oN, oY, oF, oU, oK1, oK2, oK3, oK4, oD, oRed, oInts, oPart, doubles;
 };
 
 struct CallArgs {
@@ -60,7 +61,7 @@ struct CallArgs {
 
 // Pointers into one CTA's shared memory.
 struct Cell {
-  double *A, *kf, *kr, *v, *n, *N, *Y, *F, *U, *K1, *K2, *K3, *K4, *dinv, *red;
+  double *A, *kf, *kr, *v, *n, *N, *Y, *F, *U, *K1, *K2, *K3, *K4, *dinv, *red, *part;
   int* ints;
 };
 
@@ -82,6 +83,7 @@ __device__ __forceinline__ Cell cell_arrays(const Net& net, double* smem) {
   c.dinv = smem + net.oD;
   c.red = smem + net.oRed;
   c.ints = (int*)(smem + net.oInts);
+  c.part = smem + net.oPart;
   return c;
 }
 
@@ -206,24 +208,31 @@ __device__ __forceinline__ double rhs(const Net& net, const Cell& c, const doubl
     c.v[r] = a - b;
   }
   group_sync(bar, gnt);
-  // S v: each thread its rows (ascending reactions) from its coalesced word stream; v[nr] = 0 pads the streams
+  // S v: each thread its pieces (ascending reactions) from its coalesced word stream into part; v[nr] = 0 pads
   const int g = gnt == net.st_threads[0] ? 0 : 1;
   const uint16_t* __restrict__ sw = net.sv[g] + gtid;
   const uint16_t* __restrict__ sr = net.sv_rows[g] + gtid;
   double s = 0.0;
-  int row = 0;
+  int piece = 0;
   const int rounds = net.sv_rounds[g];
 #pragma unroll 4
   for (int q = 0; q < rounds; q++) {
     const unsigned w = __ldg(sw + q * gnt);
     s = fma(code_coefficient(w >> 11), c.v[w & 0x7ffu], s);
     if (w & 0x2000u) {
-      const int i = __ldg(sr + row * gnt);
-      c.F[i] = s * ixf;
-      if (u0) c.U[i] = s / nd;
+      c.part[__ldg(sr + piece * gnt)] = s;
       s = 0.0;
-      row++;
+      piece++;
     }
+  }
+  group_sync(bar, gnt);
+  // each row: its pieces added in order
+  for (int i = gtid; i < ns; i += gnt) {
+    const int p0 = __ldg(net.sv_row_ptr + i), p1 = __ldg(net.sv_row_ptr + i + 1);
+    double r = c.part[p0];
+    for (int p = p0 + 1; p < p1; p++) r += c.part[p];
+    c.F[i] = r * ixf;
+    if (u0) c.U[i] = r / nd;
   }
   group_sync(bar, gnt);
   return ntot;

@@ -677,6 +677,7 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   net.oD = take(ns);
   net.oRed = take(8);
   net.oInts = take((ns + 8) / 2 + 1);
+  net.oPart = take(n->n_pieces);
   net.doubles = off;
   s->smem = (size_t)off * sizeof(double);
 
@@ -727,6 +728,8 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   if (e == cudaSuccess) e = upload(s, n->jac_ptr, n->n_entries + 1, &net.jac_ptr);
   if (e == cudaSuccess) e = upload(s, n->jac_entry, n->n_entries, &net.jac_entry);
   if (e == cudaSuccess) e = upload(s, n->jac_term, njt, &net.jac_term);
+  net.n_pieces = n->n_pieces;
+  if (e == cudaSuccess) e = upload(s, n->sv_row_ptr, ns + 1, &net.sv_row_ptr);
   for (int g = 0; g < 2 && e == cudaSuccess; g++) {
     const int t = n->stream_threads[g];
     net.st_threads[g] = t;

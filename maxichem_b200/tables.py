@@ -256,20 +256,35 @@ def _balance(sizes: list[int], threads: int) -> list[list[int]]:
     return lanes
 
 
-def thread_streams(tab: Tables, threads: int) -> dict[str, np.ndarray]:
-    """Each thread's S v rows and Jacobian entries as coalesced word streams (word q of thread t at q * threads + t).
+def sv_pieces(tab: Tables) -> tuple[int, np.ndarray, list[list[int]]]:
+    """The S v rows cut into pieces: the piece length P (a property of the network: the terms over 128 threads, at
+    least 8), each row's first piece (int32 [ns + 1]) and each piece's terms. Row i's sum is its pieces' sums added in
+    order, each piece summed in ascending reaction order from 0; a row with no terms has one empty piece (sum 0)."""
+    total = int(len(tab.sv_term))
+    P = max(8, -(-total // 128))
+    ptr, pieces = [0], []
+    for i in range(tab.ns):
+        terms = list(range(int(tab.sv_ptr[i]), int(tab.sv_ptr[i + 1])))
+        chunks = [terms[c : c + P] for c in range(0, len(terms), P)] or [[]]
+        pieces.extend(chunks)
+        ptr.append(len(pieces))
+    return P, np.array(ptr, np.int32), pieces
 
-    S v: a thread sums its rows one after the other, each in ascending reaction order; a word is the reaction
-    (11 bits; nr is the zero padding), the coefficient code << 11 and SV_END on a row's last term; sv_rows lists its
-    rows. Jacobian: a thread forms its entries one after the other, each in its term order; a word is the rate index
-    | code << 12 | J_END | a << 16 | b << 24, padding rate 2 nr (a zero) with a = b = ns; jac_dst lists the dense index
-    p ld + q of its entries, ld = ns | 1. The order of every sum is the plain one, so the bits do not change.
+
+def thread_streams(tab: Tables, threads: int) -> dict[str, np.ndarray]:
+    """Each thread's S v pieces and Jacobian entries as coalesced word streams (word q of thread t at q * threads + t).
+
+    S v: a thread sums its pieces (sv_pieces) one after the other; a word is the reaction (11 bits; nr is the zero
+    padding), the coefficient code << 11 and SV_END on a piece's last term; sv_rows lists the pieces it writes (their
+    index into the row-ordered piece list). Jacobian: a thread forms its entries one after the other, each in its term
+    order; a word is the rate index | code << 12 | J_END | a << 16 | b << 24, padding rate 2 nr (a zero) with a = b =
+    ns; jac_dst lists the dense index p ld + q of its entries, ld = ns | 1. Every sum keeps its order.
     """
     ns, nr = tab.ns, tab.nr
     ld = ns | 1
-    rows = [list(range(tab.sv_ptr[i], tab.sv_ptr[i + 1])) for i in range(ns)]
-    by_thread = _balance([len(r) for r in rows], threads)
-    rounds = max(1, max(sum(len(rows[i]) for i in its) for its in by_thread))
+    _, _, pieces = sv_pieces(tab)
+    by_thread = _balance([max(1, len(pc)) for pc in pieces], threads)
+    rounds = max(1, max(sum(max(1, len(pieces[i])) for i in its) for its in by_thread))
     nrow = max(1, max(len(its) for its in by_thread))
     sv = np.full((rounds, threads), nr, np.uint16)
     sv_rows = np.zeros((nrow, threads), np.uint16)
@@ -277,9 +292,12 @@ def thread_streams(tab: Tables, threads: int) -> dict[str, np.ndarray]:
         q = 0
         for e, i in enumerate(its):
             sv_rows[e, t] = i
-            for n, term in enumerate(rows[i]):
+            if not pieces[i]:  # a species in no reaction (an inert bath gas): one zero word writes its sum 0
+                sv[q, t] = nr | SV_END
+                q += 1
+            for n, term in enumerate(pieces[i]):
                 w = int(tab.sv_term[term])
-                sv[q, t] = (w & 0xFFFF) | ((w >> 16) & 3) << 11 | (SV_END if n == len(rows[i]) - 1 else 0)
+                sv[q, t] = (w & 0xFFFF) | ((w >> 16) & 3) << 11 | (SV_END if n == len(pieces[i]) - 1 else 0)
                 q += 1
     terms = [list(range(tab.jac_ptr[e], tab.jac_ptr[e + 1])) for e in range(len(tab.jac_entry))]
     by_thread = _balance([len(t) for t in terms], threads)
@@ -298,6 +316,12 @@ def thread_streams(tab: Tables, threads: int) -> dict[str, np.ndarray]:
                 jt[q, t] = (w & 0x3FFF) | (J_END if m == len(terms[e]) - 1 else 0) | (w & 0xFFFF0000)
                 q += 1
     return {"sv": sv, "sv_rows": sv_rows, "jt": jt, "jac_dst": jd}
+
+
+def sv_row_pieces(tab: Tables) -> tuple[int, np.ndarray]:
+    """The piece length and each row's first piece, for the kernels and the oracle."""
+    P, ptr, _ = sv_pieces(tab)
+    return P, ptr
 
 
 def work_counts(tab: Tables) -> dict[str, float]:

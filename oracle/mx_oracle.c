@@ -166,11 +166,19 @@ static double rhs(const cellctx* c, const double* Y, double* F, double* u0, doub
     c->v[r] = a - b;
   }
   static const double code[4] = {1.0, -1.0, 2.0, -2.0};
+  /* row i: its terms in pieces of sv_piece, each summed from 0 in ascending reaction order, the pieces added in order */
+  const int P = net->sv_piece;
   for (int i = 0; i < ns; i++) {
     double s = 0.0;
-    for (int t = net->sv_ptr[i]; t < net->sv_ptr[i + 1]; t++) {
-      const uint32_t w = net->sv_term[t];
-      s = fma(code[(w >> 16) & 3], c->v[w & 0xffff], s);
+    const int t0 = net->sv_ptr[i], t1 = net->sv_ptr[i + 1];
+    for (int c0 = t0; c0 < t1 || c0 == t0; c0 += P) {
+      double part = 0.0;
+      for (int t = c0; t < t1 && t < c0 + P; t++) {
+        const uint32_t w = net->sv_term[t];
+        part = fma(code[(w >> 16) & 3], c->v[w & 0xffff], part);
+      }
+      s = c0 == t0 ? part : s + part;
+      if (t1 == t0) break;
     }
     F[i] = s * ixf;
     if (u0) u0[i] = s / nd;
