@@ -33,6 +33,10 @@ NETWORK = "chno69"
 LEVELS = 64
 SPINUP_CALLS = 4
 DT = 300.0
+# DRAM bytes of one call-kernel launch per cell: ncu's dram__bytes_read.sum + dram__bytes_write.sum of the timed call
+# at 262,144 cells (424.33 MB), divided by its cells; a launch's traffic grows with its cells.
+TRAFFIC_PER_CELL = 424.33e6 / 262144
+HBM_GBS = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"] if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
 
 
 def parse() -> argparse.Namespace:
@@ -42,7 +46,9 @@ def parse() -> argparse.Namespace:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--cells", type=int, default=1 << 20, help="cells per GPU")
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    p.add_argument("--cpu-sample", type=int, default=131072, help="cells of the CPU baseline sample")
+    p.add_argument("--cpu-sample", type=int, default=262144, help="cells of the CPU baseline sample")
+    p.add_argument("--ref-sample", type=int, default=16384,
+                   help="cells of the reference arm's sample (its four spin-up calls run on the CPU too)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -107,7 +113,7 @@ def run_reference(args) -> None:
     net = synthetic.network(NETWORK)
     tab = tables.build(net, True)
     ref = oracle.Oracle(tab)
-    sample = min(args.cpu_sample, args.cells)
+    sample = min(args.ref_sample, args.cells)
     w = inputs(net, sample, seed=7)
     x, h = w.x, w.h
     for _ in range(SPINUP_CALLS):
@@ -142,12 +148,10 @@ def main() -> None:
     import torch
     import torch.distributed as dist
 
-    from maxichem_b200 import abi, synthetic
+    from maxichem_b200 import abi, replicas, synthetic
     from maxichem_b200.solver import CudaSolver, check_inputs
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, local, world = replicas.rank_from_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
@@ -156,7 +160,7 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
     net = synthetic.network(NETWORK)
     B = args.cells
-    w = inputs(net, B, seed=1000 + rank)  # each rank its own shard of columns
+    w = inputs(net, B, seed=replicas.seed(1000, rank))  # each rank its own batch of columns (weak scaling)
     t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
     solver = CudaSolver(net, dev, photo=True)
     tab = solver.tab
@@ -191,24 +195,23 @@ def main() -> None:
             ends[k].record(stream)
         e_all1.record(stream)
         torch.cuda.synchronize(dev)
-    total_ms = e_all0.elapsed_time(e_all1)
+    total_ms = replicas.max_over_ranks(e_all0.elapsed_time(e_all1), dev)  # the slowest rank's device time
     if world > 1:
-        m = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        total_ms = float(m.item())
         dist.barrier()
     ms = total_ms / args.steps
-    counts = solver.count.cpu().tolist()
+    counts = replicas.sum_counts(solver.count).cpu().tolist()  # every rank's cells
     nt = tries.cpu().tolist()
     phases = phase_shares(solver, lib, x, T, P, dt, h, J, dev)
     steps_mean = float(out["steps"].mean())
-    value = world * B / (ms * 1e-3)
+    value = replicas.throughput(B, world, ms * 1e-3)
     # roofline: algorithmic FP64 work of the call kernel per launch / its time (events on the launching stream)
     f = tab.flops
     fresh, retry = nt[0] - nt[1], nt[1]
     flop_step = (fresh * f["fresh_try"] + retry * f["retry"] + B * f["rates"]) / args.steps
     peak = ctypes_probe(lib, local)
     achieved = flop_step / (ms * 1e-3) / 1e12
+    # the call's HBM I/O: x, T, P, dt, h, J in; x, h, steps (f64) and done, flag, status (int32) out
+    io_bytes = B * (8 * (2 * tab.ns + tab.nj + 6) + 12)
     line = {
         "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -221,7 +224,10 @@ def main() -> None:
                    "counts": dict(zip(["queue", *abi_counts()], counts)), "spinup": spin, "layout": solver.info,
                    "phase_shares": phases},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak / 1e3, "unit": "TFLOP/s",
-                     "frac": achieved / (peak / 1e3) if peak else None, "traffic": None,
+                     "frac": achieved / (peak / 1e3) if peak else None, "traffic": TRAFFIC_PER_CELL * B,
+                     "traffic_source": "ncu DRAM bytes of the call kernel at 262,144 cells, scaled by cells",
+                     "algorithmic_bytes": io_bytes, "hbm_gbs": io_bytes / (ms * 1e-3) / 1e9,
+                     "hbm_frac_of_measured": io_bytes / (ms * 1e-3) / 1e9 / HBM_GBS,
                      "peak_source": "measured in-process: FP64 fma chains on every SM (mx_probe_fp64)",
                      "flops_per_step": flop_step},
         "gpu_launches": 3 * args.steps,
@@ -229,6 +235,8 @@ def main() -> None:
     }  # fmt: skip
     if not args.no_e2e:
         line["e2e"] = e2e(solver, x, h, w, dev, args)
+        line["e2e"]["ms_per_step"] = replicas.max_over_ranks(line["e2e"]["ms_per_step"], dev)
+        line["e2e"]["value"] = replicas.throughput(B, world, line["e2e"]["ms_per_step"] * 1e-3)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(tab, x, h, w, args)
     solver.close()

@@ -7,8 +7,8 @@
  * reference's Python surface on top of these entry points through ctypes.
  *
  * Conventions: all array arguments of mx_call are DEVICE pointers on the solver's device, row-major, float64 unless
- * stated; nothing is allocated per call; errors come back as a nonzero status and a message in err (never an
- * exception across the ABI). Inputs and outputs must not alias. Calls on one solver run one at a time on the given
+ * stated; a call allocates nothing except when its B exceeds every earlier call's (the solver's recompute list then
+ * grows, once); errors come back as a nonzero status and a message in err (never an exception across the ABI). Inputs and outputs must not alias. Calls on one solver run one at a time on the given
  * stream (its scratch, queues and list are shared), as the reference's do (maxichem/kincuda.py:114-116).
  */
 #ifndef MAXICHEM_B200_H
