@@ -132,6 +132,27 @@ int mx_call(mx_solver* s, const double* x, const double* T, const double* P, con
             int32_t* done, double* steps, int32_t* flag, int32_t* status, int32_t* count, int64_t* total,
             void* stream, char* err, size_t errlen);
 
+/* Cells of one mx_call_static call at most: the size of its static recompute list (4 MiB of device memory). */
+#define MX_STATIC_MAX_CELLS 1048576
+
+/*
+ * mx_call for callers that cannot allocate device memory. No counterpart in the reference. Same arguments, results,
+ * errors and kernels as mx_call, but the call's only scratch (the recompute list, one int32 per cell) is a file-scope
+ * static device array of MX_STATIC_MAX_CELLS entries instead of solver-owned memory, so the call never calls
+ * cudaMalloc, cudaFree or any allocating library routine (the solver handle itself still comes from mx_create).
+ * - B above MX_STATIC_MAX_CELLS is refused with MX_ERR_ARGUMENT and a message naming the limit.
+ * - The first call on a device looks up the array's address there (cudaGetSymbolAddress, with that device current)
+ *   and keeps it; make that first call before any stream capture on the device.
+ * - Every call of every solver in the process shares the array, which keeps the last call's contents. Nothing in it
+ *   must start at zero (a call writes each entry before reading it); the queue and list counters that must start at
+ *   zero are in count, which the call clears. Calls that overlap on the GPU (other streams, other threads) race on
+ *   the array: run them one after another.
+ */
+int mx_call_static(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
+                   const double* h_in, const double* J, int64_t B, double rtol, double atol, int32_t max_steps,
+                   double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag, int32_t* status,
+                   int32_t* count, int64_t* total, void* stream, char* err, size_t errlen);
+
 /* The guard alone on given states (replaces a launch of the reference's guard kernel, maxichem/kernels/guard.cuh:114):
  * counts refused cells from status, checks and corrects the others in x_out, writes flag 0/1 and the recompute list
  * count. Device pointers; used by tests of the guard's thresholds. */

@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -932,6 +933,100 @@ extern "C" int mx_probe_fp64(int device, int64_t iters, double* gflops) {
   cudaFree(out);
   if (e != cudaSuccess || ms <= 0.0f) return MX_ERR_CUDA;
   *gflops = 2.0 * 8.0 * (double)iters * blocks * threads / (ms * 1e-3) / 1e9;
+  return MX_OK;
+}
+
+// ---- mx_call_static: the call for callers that cannot allocate device memory ----
+// The only scratch a call owns is the recompute list (one int per cell). Here it is a file-scope device array of
+// MX_STATIC_MAX_CELLS entries that every mx_call_static call shares; its address on a device is looked up once, at
+// that device's first call, with the device current.
+
+static __device__ __align__(256) int g_static_list[MX_STATIC_MAX_CELLS];
+
+namespace {
+
+constexpr int MAX_DEVICES = 64;
+int* g_static_list_ptr[MAX_DEVICES] = {};
+std::mutex g_static_mutex;
+
+int static_list(int device, int** out, char* err, size_t errlen) {
+  if (device < 0 || device >= MAX_DEVICES) {
+    set_error(err, errlen, "mx_call_static: device %d out of range", device);
+    return MX_ERR_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_list_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_list);
+    if (e != cudaSuccess || !p) {
+      set_error(err, errlen, "mx_call_static: the static scratch's address on device %d: %s", device,
+                cudaGetErrorString(e));
+      return MX_ERR_CUDA;
+    }
+    g_static_list_ptr[device] = static_cast<int*>(p);
+  }
+  *out = g_static_list_ptr[device];
+  return MX_OK;
+}
+
+}  // namespace
+
+extern "C" int mx_call_static(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
+                              const double* h_in, const double* J, int64_t B, double rtol, double atol,
+                              int32_t max_steps, double* x_out, double* h_out, int32_t* done, double* steps,
+                              int32_t* flag, int32_t* status, int32_t* count, int64_t* total, void* stream, char* err,
+                              size_t errlen) {
+  if (!s) {
+    set_error(err, errlen, "this solver was closed; build a new one");
+    return MX_ERR_CLOSED;
+  }
+  if (B < 0 || B > MX_STATIC_MAX_CELLS) {
+    set_error(err, errlen, "mx_call_static: B = %lld cells; from 0 to MX_STATIC_MAX_CELLS = %d expected (use mx_call "
+              "for larger batches)", (long long)B, MX_STATIC_MAX_CELLS);
+    return MX_ERR_ARGUMENT;
+  }
+  if (!(rtol > 0.0 && rtol < 1e300 && atol > 0.0 && atol < 1e300)) {
+    set_error(err, errlen, "rtol and atol finite and positive expected, got %g, %g", rtol, atol);
+    return MX_ERR_ARGUMENT;
+  }
+  if (max_steps < 1 || (int64_t)MX_REC_STEPS * max_steps > 0x7fffffff) {
+    set_error(err, errlen, "max_steps from 1 to %d expected, got %d", 0x7fffffff / MX_REC_STEPS, max_steps);
+    return MX_ERR_ARGUMENT;
+  }
+  if (!count || !total || (B > 0 && (!x || !T || !P || !dt || !h_in || !x_out || !h_out || !done || !steps ||
+                                     !flag || !status || (s->net.nj > 0 && !J)))) {
+    set_error(err, errlen, "mx_call_static: a required array is null");
+    return MX_ERR_ARGUMENT;
+  }
+  DeviceScope scope(s->device);
+  if (scope.status != cudaSuccess) {
+    set_error(err, errlen, "mx_call_static: device %d: %s", s->device, cudaGetErrorString(scope.status));
+    return MX_ERR_CUDA;
+  }
+  int* list = nullptr;
+  const int rc = static_list(s->device, &list, err, errlen);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // count holds the cell queue and the list's length: both must start at zero. The list itself needs no clearing:
+  // a call writes each entry before its recovery kernel reads it.
+  cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
+  if (e == cudaSuccess && B > 0) {
+    CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status, count,
+               list, s->tries};
+    const int grid = (int)std::min<int64_t>(B, (int64_t)s->call_ctas * s->sms);
+    s->call<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, nullptr);
+    const int rgrid = (int)std::min<int64_t>(B, (int64_t)s->recover_ctas * s->sms);
+    s->recover<<<rgrid, 32 * WARPS, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    add_counts_kernel<<<1, 32, 0, st>>>(count, (long long*)total);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_call_static: %s", cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
   return MX_OK;
 }
 
