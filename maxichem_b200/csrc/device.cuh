@@ -44,7 +44,7 @@ struct Net {
   const uint32_t* jt[2];
   const uint16_t* jd[2];
   // shared-memory layout
-  int ld, oA, oK, oV, on, oN, oY, oF, oU, oK1, oK2, oK3, oK4, oD, oRed, oInts, oPart, doubles;
+  int ld, oA, oK, oV, on, oN, oY, oF, oU, oK1, oK2, oK3, oK4, oD, oRed, oInts, oPart, oG, doubles;
 };
 
 struct CallArgs {
@@ -61,7 +61,7 @@ struct CallArgs {
 
 // Pointers into one CTA's shared memory.
 struct Cell {
-  double *A, *kf, *kr, *v, *n, *N, *Y, *F, *U, *K1, *K2, *K3, *K4, *dinv, *red, *part;
+  double *A, *kf, *kr, *v, *n, *N, *Y, *F, *U, *K1, *K2, *K3, *K4, *dinv, *red, *part, *G;
   int* ints;
 };
 
@@ -84,6 +84,7 @@ __device__ __forceinline__ Cell cell_arrays(const Net& net, double* smem) {
   c.red = smem + net.oRed;
   c.ints = (int*)(smem + net.oInts);
   c.part = smem + net.oPart;
+  c.G = smem + net.oG;
   return c;
 }
 
@@ -605,97 +606,103 @@ __device__ void try_error(const Net& net, const Cell& c, bool first, double rtol
 // Sums over species are formed as a warp forms them: lane l adds species l, l + 32, ... in order, then the butterfly.
 // The small element system (at most MX_MAX_ELEMENTS) is factored by every lane alike from the butterflied sums.
 
-// sum over species of f(i) in the warp's order (every lane returns it)
-template <typename F>
-__device__ __forceinline__ double species_sum(int ns, int lane, F f) {
-  double p = 0.0;
-  for (int i = lane; i < ns; i += 32) p = f(i, p);
-  return warp_sum(p);
+// Doubles of shared scratch the guard needs (guard_scratch): e0 and e1, the element matrix, its first diagonal, the
+// right side, lambda, the sum, and g per species.
+__host__ __device__ constexpr int guard_scratch(int ns) {
+  return 2 * MX_MAX_ELEMENTS + MX_MAX_ELEMENTS * MX_MAX_ELEMENTS + 3 * MX_MAX_ELEMENTS + 2 + ns;
 }
 
-// Guard bits of a stepped cell's result xo (network order, shared memory) against its input x0; a passing result
-// has its element shares put back in place (check_cell): x' = x (1 + sum_e lambda_e a_ie), clamped, renormalised.
-// Every lane of the warp returns the bits.
+// The guard's test of a stepped cell's result xo (network species order) against its input x0, on one warp: the bits
+// GUARD_NONFINITE, GUARD_UNFINISHED, GUARD_DRIFT, 0 when it passed (guard.cuh:63-108). A passing result has its element
+// shares put back in place (element_multipliers, guard.cuh:24-57): x' = x (1 + sum_e lambda_e a_ie), clamped,
+// renormalised. Every sum runs over the species in network order, one lane per sum, as the reference's one thread
+// per cell adds them, so each sum has the reference's bits. at: atoms [ns][nel]; scr: guard_scratch(ns) doubles of
+// shared memory, free during the guard.
 __device__ __noinline__ int check_cell(const Net& net, const double* x0, double* xo, int done, double nok,
-                                       double atol, int lane, const double* at) {
+                                       double atol, int lane, const double* at, double* scr) {
+  constexpr int ME = MX_MAX_ELEMENTS;
   const int ns = net.ns, nel = net.nel;
-  double e0[MX_MAX_ELEMENTS], e1[MX_MAX_ELEMENTS];
-  double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-  for (int e = 0; e < MX_MAX_ELEMENTS; e++) {
-    e0[e] = e1[e] = 0.0;
-    if (e < nel) {
-      e0[e] = species_sum(ns, lane, [&](int i, double p) { return fma(at[i * nel + e], x0[i], p); });
-      e1[e] = species_sum(ns, lane, [&](int i, double p) { return fma(at[i * nel + e], xo[i], p); });
-      s0 += e0[e];
-      s1 += e1[e];
-    }
+  double* se = scr;            // [2 ME]: e0, then e1 at ME
+  double* m = se + 2 * ME;     // [ME][ME], upper triangle
+  double* m0 = m + ME * ME;    // [ME]
+  double* y = m0 + ME;         // [ME]
+  double* lam = y + ME;        // [ME]
+  double* sum_at = lam + ME;   // [2]
+  double* g = sum_at + 2;      // [ns]
+  if (lane < 2 * nel) {        // e0[e] on lanes 0..nel-1, e1[e] on lanes nel..2 nel-1 (guard.cuh:70-77)
+    const int e = lane < nel ? lane : lane - nel;
+    const double* xs = lane < nel ? x0 : xo;
+    double acc = 0.0;
+    for (int i = 0; i < ns; i++) acc = fma(at[i * nel + e], xs[i], acc);
+    se[lane < nel ? e : ME + e] = acc;
   }
   bool fin = true;
   for (int i = lane; i < ns; i += 32) fin = fin && isfinite(xo[i]);
   const bool xfin = __all_sync(FULL, fin);
-  bool drift = false;
-#pragma unroll
-  for (int e = 0; e < MX_MAX_ELEMENTS; e++)
-    if (e < nel)
-      drift = drift || fabs(e1[e] / s1 - e0[e] / s0) > net.drift * e0[e] / s0 + 2.0 * atol * nok * net.etot / s0;
+  __syncwarp();
+  double s0 = 0.0, s1 = 0.0;
+  for (int e = 0; e < nel; e++) {
+    s0 += se[e];
+    s1 += se[ME + e];
+  }
+  bool drift = false;  // shares_drifted (guard.cuh:13-21)
+  for (int e = 0; e < nel; e++)
+    drift = drift || fabs(se[ME + e] / s1 - se[e] / s0) > net.drift * se[e] / s0 + 2.0 * atol * nok * net.etot / s0;
   const int c = (xfin ? 0 : GUARD_NONFINITE) | (done ? 0 : GUARD_UNFINISHED) | (drift ? GUARD_DRIFT : 0);
   if (c) return c;
-  // lambda of (A X A^T) lambda = e0 s1 / s0 - e1 by LDL^T; an element whose pivot vanishes is left out
-  double m[MX_MAX_ELEMENTS * MX_MAX_ELEMENTS], m0[MX_MAX_ELEMENTS], y[MX_MAX_ELEMENTS], lam[MX_MAX_ELEMENTS];
-  const double r = s1 / s0;
-#pragma unroll
-  for (int e = 0; e < MX_MAX_ELEMENTS; e++) {
-#pragma unroll
-    for (int f = 0; f < MX_MAX_ELEMENTS; f++) {
-      m[e * MX_MAX_ELEMENTS + f] = 0.0;
-      if (e < nel && f < nel && f >= e)
-        m[e * MX_MAX_ELEMENTS + f] = species_sum(ns, lane, [&](int i, double p) {
-          const double ae = at[i * nel + e], af = at[i * nel + f];
-          return (ae != 0.0 && af != 0.0) ? fma(ae * af, xo[i], p) : p;
-        });
-    }
-    m0[e] = m[e * MX_MAX_ELEMENTS + e];
-    y[e] = e < nel ? fma(e0[e], r, -e1[e]) : 0.0;
-  }
-#pragma unroll
-  for (int k = 0; k < MX_MAX_ELEMENTS; k++) {
-    if (k >= nel || !(m[k * MX_MAX_ELEMENTS + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
-#pragma unroll
-    for (int j = k + 1; j < MX_MAX_ELEMENTS; j++) {
-      if (j >= nel) continue;
-      const double l = m[k * MX_MAX_ELEMENTS + j] / m[k * MX_MAX_ELEMENTS + k];
-#pragma unroll
-      for (int f = j; f < MX_MAX_ELEMENTS; f++)
-        if (f < nel) m[j * MX_MAX_ELEMENTS + f] = fma(-l, m[k * MX_MAX_ELEMENTS + f], m[j * MX_MAX_ELEMENTS + f]);
-      y[j] = fma(-l, y[k], y[j]);
+  // (A X A^T)[e][f], f >= e: over species with a_ie and a_if both nonzero (guard.cuh:29-37)
+  for (int q = lane; q < nel * nel; q += 32) {
+    const int e = q / nel, f = q - e * nel;
+    if (f >= e) {
+      double acc = 0.0;
+      for (int i = 0; i < ns; i++) {
+        const double ae = at[i * nel + e], af = at[i * nel + f];
+        if (ae != 0.0 && af != 0.0) acc = fma(ae * af, xo[i], acc);
+      }
+      m[e * ME + f] = acc;
     }
   }
-#pragma unroll
-  for (int k = MX_MAX_ELEMENTS - 1; k >= 0; k--) {
-    lam[k] = 0.0;
-    if (k >= nel || !(m[k * MX_MAX_ELEMENTS + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
-    double b = y[k];
-#pragma unroll
-    for (int f = k + 1; f < MX_MAX_ELEMENTS; f++)
-      if (f < nel) b = fma(-m[k * MX_MAX_ELEMENTS + f], lam[f], b);
-    lam[k] = b / m[k * MX_MAX_ELEMENTS + k];
-  }
-  double part = 0.0;
-  for (int i = lane; i < ns; i += 32) {
-    double g = 1.0;
-#pragma unroll
-    for (int e = 0; e < MX_MAX_ELEMENTS; e++) {
-      if (e < nel) {
-        const double a = at[i * nel + e];
-        if (a != 0.0) g = fma(lam[e], a, g);
+  __syncwarp();
+  if (lane == 0) {  // LDL^T and the back substitution; an element whose pivot vanishes is left out (guard.cuh:38-56)
+    const double r = s1 / s0;
+    for (int e = 0; e < nel; e++) {
+      m0[e] = m[e * ME + e];
+      y[e] = fma(se[e], r, -se[ME + e]);
+    }
+    for (int k = 0; k < nel; k++) {
+      if (!(m[k * ME + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
+      for (int j = k + 1; j < nel; j++) {
+        const double l = m[k * ME + j] / m[k * ME + k];
+        for (int f = j; f < nel; f++) m[j * ME + f] = fma(-l, m[k * ME + f], m[j * ME + f]);
+        y[j] = fma(-l, y[k], y[j]);
       }
     }
-    g = fmin(fmax(g, 1.0 - MX_GMAX), 1.0 + MX_GMAX);
-    part = fma(xo[i], g, part);
-    xo[i] *= g;
+    for (int k = nel - 1; k >= 0; k--) {
+      lam[k] = 0.0;
+      if (!(m[k * ME + k] > MX_ELEMENT_PIVOT_MIN * m0[k])) continue;
+      double b = y[k];
+      for (int f = k + 1; f < nel; f++) b = fma(-m[k * ME + f], lam[f], b);
+      lam[k] = b / m[k * ME + k];
+    }
   }
-  const double sum = warp_sum(part);
+  __syncwarp();
+  for (int i = lane; i < ns; i += 32) {  // g per species (guard.cuh:94-99)
+    double gi = 1.0;
+    for (int e = 0; e < nel; e++) {
+      const double a = at[i * nel + e];
+      if (a != 0.0) gi = fma(lam[e], a, gi);
+    }
+    g[i] = fmin(fmax(gi, 1.0 - MX_GMAX), 1.0 + MX_GMAX);
+  }
+  __syncwarp();
+  if (lane == 0) {  // the sum of x g in network order (guard.cuh:100)
+    double sum = 0.0;
+    for (int i = 0; i < ns; i++) sum = fma(xo[i], g[i], sum);
+    sum_at[0] = sum;
+  }
+  __syncwarp();
+  const double sum = sum_at[0];
+  for (int i = lane; i < ns; i += 32) xo[i] *= g[i];
   __syncwarp();
   if (!(isfinite(sum) && sum > 0.0)) return GUARD_NONFINITE;
   const double is = 1.0 / sum;

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const Ca
     __syncthreads();
     if (warp == 0) {
       const int done = (st == 0 && s.t >= dt * MX_CALL_END) ? 1 : 0;
-      const int g = st == 0 ? check_cell(net, xin, c.Y, done, s.nok, a.atol, lane, at) : 0;
+      const int g = st == 0 ? check_cell(net, xin, c.Y, done, s.nok, a.atol, lane, at, c.G) : 0;
       if (lane == 0) {
         a.h_out[cell] = s.h;
         a.done[cell] = done;
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(32 * W, 4) recover_kernel(const Net net, const
       __syncthreads();
       if (warp == 0) {
         const int dn = s.t >= dt * MX_CALL_END ? 1 : 0;
-        const int g = check_cell(net, xin, c.Y, dn, s.nok, a.atol, lane, at);
+        const int g = check_cell(net, xin, c.Y, dn, s.nok, a.atol, lane, at, c.G);
         if (lane != 0) {
         } else if (g == GUARD_DRIFT && k < MX_REC_RETRIES) {
           c.ints[1] = -1;  // only the element test failed: again from the inputs with a smaller first try
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(32 * W, 4) time_phases_kernel(const Net net, c
       for (int i = lane; i < ns; i += 32) c.Y[__ldg(net.perm + i)] = c.N[i];
       __syncwarp();
       t = clock64();
-      check_cell(net, x0, c.Y, 1, 1.0, 1e-25, lane, net.atoms);
+      check_cell(net, x0, c.Y, 1, 1.0, 1e-25, lane, net.atoms, c.G);
       u = clock64();
       acc[8] += u - t;
     }
@@ -494,11 +494,13 @@ __global__ void __launch_bounds__(32 * W, 4) time_phases_kernel(const Net net, c
 __global__ void __launch_bounds__(128) guard_kernel(const Net net, const double* x0, double* xout, const int* done,
                                                     const double* nok, const int* status, int B, double atol,
                                                     int* flag, int* count, int* list) {
+  extern __shared__ double gsm[];  // guard_scratch(ns) doubles per warp
   const int cell = (int)(blockIdx.x * 4 + (threadIdx.x >> 5)), lane = (int)(threadIdx.x & 31);
   if (cell >= B) return;
   const int s = status[cell];
+  double* scr = gsm + (threadIdx.x >> 5) * guard_scratch(net.ns);
   const int g = s == 0 ? check_cell(net, x0 + (size_t)cell * net.ns, xout + (size_t)cell * net.ns, done[cell],
-                                    nok[cell], atol, lane, net.atoms)
+                                    nok[cell], atol, lane, net.atoms, scr)
                        : 0;
   if (lane != 0) return;
   int r = 0;
@@ -679,6 +681,13 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   net.oRed = take(8);
   net.oInts = take((ns + 8) / 2 + 1);
   net.oPart = take(n->n_pieces);
+  {  // the guard's scratch: in the matrix's space past the staged atoms and input row when it fits there
+    const int staged = (ns * n->nel + ns + 1) & ~1;
+    if (staged + guard_scratch(ns) <= ns * net.ld)
+      net.oG = net.oA + staged;
+    else
+      net.oG = take(guard_scratch(ns));
+  }
   net.doubles = off;
   s->smem = (size_t)off * sizeof(double);
 
@@ -837,8 +846,9 @@ extern "C" int mx_guard(mx_solver* s, const double* x, double* x_out, const int3
   if (rc) return rc;
   cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
   if (e == cudaSuccess && B > 0) {
-    guard_kernel<<<(int)((B + 3) / 4), 128, 0, st>>>(s->net, x, x_out, done, steps, status, (int)B, atol, flag,
-                                                          count, s->list);
+    const size_t gsmem = 4 * sizeof(double) * guard_scratch(s->net.ns);
+    guard_kernel<<<(int)((B + 3) / 4), 128, gsmem, st>>>(s->net, x, x_out, done, steps, status, (int)B, atol, flag,
+                                                              count, s->list);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) {

@@ -291,48 +291,47 @@ static void sherman(int ns, double* y, const double* u, double c0) {
 }
 
 /* ---- guard (guard.cuh:13-108) ----
- * Sums over species in the warp's order (lane l: species l, l + 32, ..., then the butterfly), as the kernel's
- * warp-parallel guard forms them; the element system is solved as the reference solves it. */
+ * Every sum runs over the species in network order, as the reference's one thread per cell adds them. */
 
 /* check_cell: guard bits of a stepped cell's result; a passing result has its element shares put back in xo. */
 int mxo_check_cell(const mx_network* net, const double* x0, double* xo, int done, double nok, double atol,
                    double drift) {
   const int ns = net->ns, nel = net->nel;
   const double* at = net->atoms;
-  double e0[MX_MAX_ELEMENTS], e1[MX_MAX_ELEMENTS], lam[MX_MAX_ELEMENTS], p[32], q[32];
+  double e0[MX_MAX_ELEMENTS], e1[MX_MAX_ELEMENTS], lam[MX_MAX_ELEMENTS];
   double etot = 0.0, s0 = 0.0, s1 = 0.0;
   for (int i = 0; i < ns * nel; i++) etot += at[i];
-  for (int e = 0; e < nel; e++) {
-    for (int l = 0; l < 32; l++) p[l] = q[l] = 0.0;
-    for (int i = 0; i < ns; i++) {
-      p[i & 31] = fma(at[i * nel + e], x0[i], p[i & 31]);
-      q[i & 31] = fma(at[i * nel + e], xo[i], q[i & 31]);
+  int xfin = 1;
+  for (int e = 0; e < nel; e++) e0[e] = e1[e] = 0.0;
+  for (int i = 0; i < ns; i++) { /* guard.cuh:70-77 */
+    xfin = xfin && isfinite(xo[i]);
+    for (int e = 0; e < nel; e++) {
+      e0[e] = fma(at[i * nel + e], x0[i], e0[e]);
+      e1[e] = fma(at[i * nel + e], xo[i], e1[e]);
     }
-    e0[e] = butterfly_sum(p);
-    e1[e] = butterfly_sum(q);
+  }
+  for (int e = 0; e < nel; e++) {
     s0 += e0[e];
     s1 += e1[e];
   }
-  int xfin = 1;
-  for (int i = 0; i < ns; i++) xfin = xfin && isfinite(xo[i]);
-  int drifted = 0;
+  int drifted = 0; /* shares_drifted, guard.cuh:13-21 */
   for (int e = 0; e < nel; e++)
     drifted = drifted || fabs(e1[e] / s1 - e0[e] / s0) > drift * e0[e] / s0 + 2.0 * atol * nok * etot / s0;
   const int c = (xfin ? 0 : GUARD_NONFINITE) | (done ? 0 : GUARD_UNFINISHED) | (drifted ? GUARD_DRIFT : 0);
   if (c) return c;
+  /* element_multipliers, guard.cuh:24-57 */
   double m[MX_MAX_ELEMENTS * MX_MAX_ELEMENTS], m0[MX_MAX_ELEMENTS], y[MX_MAX_ELEMENTS];
+  for (int e = 0; e < nel * nel; e++) m[e] = 0.0;
+  for (int i = 0; i < ns; i++) {
+    const double* ai = at + i * nel;
+    for (int e = 0; e < nel; e++) {
+      if (ai[e] == 0.0) continue;
+      for (int f = e; f < nel; f++)
+        if (ai[f] != 0.0) m[e * nel + f] = fma(ai[e] * ai[f], xo[i], m[e * nel + f]);
+    }
+  }
   const double r = s1 / s0;
   for (int e = 0; e < nel; e++) {
-    for (int f = 0; f < nel; f++) {
-      m[e * nel + f] = 0.0;
-      if (f < e) continue;
-      for (int l = 0; l < 32; l++) p[l] = 0.0;
-      for (int i = 0; i < ns; i++) {
-        const double ae = at[i * nel + e], af = at[i * nel + f];
-        if (ae != 0.0 && af != 0.0) p[i & 31] = fma(ae * af, xo[i], p[i & 31]);
-      }
-      m[e * nel + f] = butterfly_sum(p);
-    }
     m0[e] = m[e * nel + e];
     y[e] = fma(e0[e], r, -e1[e]);
   }
@@ -351,17 +350,16 @@ int mxo_check_cell(const mx_network* net, const double* x0, double* xo, int done
     for (int f = k + 1; f < nel; f++) b = fma(-m[k * nel + f], lam[f], b);
     lam[k] = b / m[k * nel + k];
   }
-  for (int l = 0; l < 32; l++) p[l] = 0.0;
+  double sum = 0.0; /* guard.cuh:93-101 */
   for (int i = 0; i < ns; i++) {
     const double* ai = at + i * nel;
     double g = 1.0;
     for (int e = 0; e < nel; e++)
       if (ai[e] != 0.0) g = fma(lam[e], ai[e], g);
     g = fmin(fmax(g, 1.0 - MX_GMAX), 1.0 + MX_GMAX);
-    p[i & 31] = fma(xo[i], g, p[i & 31]);
+    sum = fma(xo[i], g, sum);
     xo[i] *= g;
   }
-  const double sum = butterfly_sum(p);
   if (!(isfinite(sum) && sum > 0.0)) return GUARD_NONFINITE;
   const double is = 1.0 / sum;
   for (int i = 0; i < ns; i++) xo[i] *= is;
