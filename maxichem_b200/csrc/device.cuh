@@ -306,7 +306,7 @@ __device__ __forceinline__ void trailing_update(double* A, int ld, int kb, int n
       for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) acc[a][b] = A[row[a] * ld + col[b]];
-#pragma unroll
+#pragma unroll 2
       for (int t = 0; t < PANEL; t++) {
         if (t < nb) {
           double l[4], u[4];
@@ -392,8 +392,9 @@ __device__ __forceinline__ double pick(const double (&a)[R], int idx) {
 // taken 32 at a time, so the pivot's value comes from a register chosen at compile time (c) and one shuffle; the next
 // column of L or U is loaded while the current pivot is applied. A lane whose row takes no update from pivot k uses
 // the multiplier 0, and fma(-0, y, a) = a for finite y. Each entry receives the one-pivot sweep's fma's in its order.
+// Not inlined: the call kernel solves at four places, and one copy of the code keeps the instruction cache warm.
 template <int R, int NV>
-__device__ __forceinline__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1,
+__device__ __noinline__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1,
                                          int lane) {
   const int ns = net.ns, ld = net.ld, last = ns - 1;
   double a[NV][R], d[R];
@@ -411,7 +412,7 @@ __device__ __forceinline__ void lu_solve(const Net& net, const double* A, const 
     double m[R];
 #pragma unroll
     for (int p = c; p < R; p++) m[p] = A[min(lane + 32 * p, last) * ld + k0];
-#pragma unroll 4
+#pragma unroll 2
     for (int k = k0; k < k1; k++) {
       double yk[NV];
 #pragma unroll
@@ -436,7 +437,7 @@ __device__ __forceinline__ void lu_solve(const Net& net, const double* A, const 
     double m[R];
 #pragma unroll
     for (int p = 0; p <= c; p++) m[p] = A[min(lane + 32 * p, last) * ld + khi];
-#pragma unroll 4
+#pragma unroll 2
     for (int k = khi; k >= klo; k--) {
       double z[NV];
 #pragma unroll
