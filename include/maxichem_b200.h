@@ -8,8 +8,9 @@
  *
  * Conventions: all array arguments of mx_call are DEVICE pointers on the solver's device, row-major, float64 unless
  * stated; a call allocates nothing except when its B exceeds every earlier call's (the solver's recompute list then
- * grows, once); errors come back as a nonzero status and a message in err (never an exception across the ABI). Inputs and outputs must not alias. Calls on one solver run one at a time on the given
- * stream (its scratch, queues and list are shared), as the reference's do (maxichem/kincuda.py:114-116).
+ * grows, once); errors come back as a nonzero status and a message in err (never an exception across the ABI).
+ * Inputs and outputs must not alias. Calls on one solver run one at a time on the given stream (its scratch, queues
+ * and list are shared), as the reference's do (maxichem/kincuda.py:114-116).
  */
 #ifndef MAXICHEM_B200_H
 #define MAXICHEM_B200_H
@@ -160,8 +161,16 @@ int mx_guard(mx_solver* s, const double* x, double* x_out, const int32_t* done, 
              const int32_t* status, int64_t B, double atol, int32_t* flag, int32_t* count, void* stream, char* err,
              size_t errlen);
 
-/* Launch layout of the solver (cells per CTA, warps per cell, CTAs per SM, shared bytes), for reports. */
+/* Launch layout of the solver, for reports: warps per cell, rows per lane of the solves, shared bytes per cell,
+ * call and recovery CTAs per SM at full occupancy, SMs, the matrix's leading dimension, the call grid's CTAs per SM
+ * (0: one CTA per cell). */
 int mx_info(const mx_solver* s, int32_t* values, int32_t n);
+
+/* The call kernel's grid for later calls: ctas_per_sm from 1 to the occupancy limit runs that many persistent CTAs per
+ * SM over the cell queue; 0 launches one CTA per cell (a static launch); -1 restores the default (the occupancy
+ * limit). Results do not depend on it. No counterpart in the reference, which picks its cells per block by
+ * recompiling (maxichem/kincuda.py:184-218); maxichem_b200/autotune.py times the choices. */
+int mx_set_grid(mx_solver* s, int32_t ctas_per_sm);
 
 /* One fresh try of one cell (device x [ns], J [nj]) at try size h, with every stage written to the device array out:
  * kf, kr [nr each], F, u0 [ns each], -Jn [ns][ns], w [ns], LU factors [ns][ns], dinv, K1, K2, K3, K4, N' [ns each],

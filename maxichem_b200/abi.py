@@ -116,6 +116,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         [_P, _P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_double, _P, _P, _P, _ERR, ctypes.c_size_t],
     ),
     "mx_info": (ctypes.c_int, [_P, _P, ctypes.c_int32]),
+    "mx_set_grid": (ctypes.c_int, [_P, ctypes.c_int32]),
     "mx_destroy": (ctypes.c_int, [_P]),
     "mx_set_try_counter": (ctypes.c_int, [_P, _P]),
     "mx_set_phase_counter": (ctypes.c_int, [_P, _P]),

@@ -589,6 +589,7 @@ struct mx_solver {
   int rows_per_lane = 0;
   size_t smem = 0;
   int sms = 0, call_ctas = 0, recover_ctas = 0;
+  int grid_ctas = -1;  // call-kernel CTAs per SM: 1..call_ctas persistent, 0 one CTA per cell; -1 call_ctas
   int* list = nullptr;
   int64_t list_capacity = 0;
   unsigned long long* tries = nullptr;
@@ -762,6 +763,14 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   return MX_OK;
 }
 
+// The call kernel's grid: persistent over the cell queue with grid_ctas CTAs per SM (the occupancy limit by
+// default), or one CTA per cell (grid_ctas 0: every CTA takes one cell and finds the queue past the batch).
+static int call_grid(const mx_solver* s, int64_t B) {
+  if (s->grid_ctas == 0) return (int)B;
+  const int per_sm = s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas;
+  return (int)std::min<int64_t>(B, (int64_t)per_sm * s->sms);
+}
+
 static int grow_list(mx_solver* s, int64_t B, char* err, size_t errlen) {
   if (B <= s->list_capacity) return MX_OK;
   if (s->list) cudaFree(s->list);
@@ -809,7 +818,7 @@ extern "C" int mx_call(mx_solver* s, const double* x, const double* T, const dou
   if (e == cudaSuccess && B > 0) {
     CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status, count,
                s->list, s->tries};
-    const int grid = (int)std::min<int64_t>(B, (int64_t)s->call_ctas * s->sms);
+    const int grid = call_grid(s, B);
     if (s->phases)
       s->call_prof<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, s->phases);
     else
@@ -860,8 +869,16 @@ extern "C" int mx_guard(mx_solver* s, const double* x, double* x_out, const int3
 
 extern "C" int mx_info(const mx_solver* s, int32_t* values, int32_t n) {
   if (!s || !values) return MX_ERR_ARGUMENT;
-  const int32_t v[] = {WARPS, s->rows_per_lane, (int32_t)s->smem, s->call_ctas, s->recover_ctas, s->sms, s->net.ld};
+  const int32_t v[] = {WARPS, s->rows_per_lane, (int32_t)s->smem, s->call_ctas, s->recover_ctas, s->sms, s->net.ld,
+                       s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas};
   for (int i = 0; i < n && i < (int)(sizeof v / sizeof v[0]); i++) values[i] = v[i];
+  return MX_OK;
+}
+
+extern "C" int mx_set_grid(mx_solver* s, int32_t ctas_per_sm) {
+  if (!s) return MX_ERR_CLOSED;
+  if (ctas_per_sm < -1 || ctas_per_sm > s->call_ctas) return MX_ERR_ARGUMENT;
+  s->grid_ctas = ctas_per_sm;
   return MX_OK;
 }
 
@@ -1023,7 +1040,7 @@ extern "C" int mx_call_static(mx_solver* s, const double* x, const double* T, co
   if (e == cudaSuccess && B > 0) {
     CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status, count,
                list, s->tries};
-    const int grid = (int)std::min<int64_t>(B, (int64_t)s->call_ctas * s->sms);
+    const int grid = call_grid(s, B);
     s->call<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, nullptr);
     const int rgrid = (int)std::min<int64_t>(B, (int64_t)s->recover_ctas * s->sms);
     s->recover<<<rgrid, 32 * WARPS, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);

@@ -24,7 +24,8 @@ __all__ = ["ATOL", "COUNTS", "DRIFT", "REC_STEPS", "T_MAX", "T_MIN", "X_SUM_TOL"
            "LaunchResult"]  # fmt: skip
 
 _ERRLEN = 1024
-INFO_FIELDS = ("warps", "rows_per_lane", "smem", "call_ctas_per_sm", "recover_ctas_per_sm", "sms", "ld")
+INFO_FIELDS = ("warps", "rows_per_lane", "smem", "call_ctas_per_sm", "recover_ctas_per_sm", "sms", "ld",
+               "grid_ctas_per_sm")
 
 
 class CallResult(NamedTuple):
@@ -224,6 +225,18 @@ class CudaSolver:
         """Advance each cell by dt: ``launch`` without the flag in its result (``self.flag`` keeps it)."""
         r = self.launch(x, T, P, dt, h, rtol=rtol, atol=atol, max_steps=max_steps, J=J)
         return CallResult(r.x, r.h, r.done, r.steps)
+
+    def set_grid(self, ctas_per_sm: int) -> None:
+        """The call kernel's grid for later calls: 1 .. info["call_ctas_per_sm"] persistent CTAs per SM over the cell
+        queue, 0 one CTA per cell, -1 the default (the occupancy limit). Results do not depend on it."""
+        self._require_open()
+        if self._lib.mx_set_grid(self._handle, int(ctas_per_sm)):
+            raise ValueError(
+                f"ctas_per_sm from -1 to {self.info['call_ctas_per_sm']} expected, got {ctas_per_sm}"
+            )
+        values = (ctypes.c_int32 * len(INFO_FIELDS))()
+        self._lib.mx_info(self._handle, values, len(INFO_FIELDS))
+        self.info["grid_ctas_per_sm"] = int(values[len(INFO_FIELDS) - 1])
 
     @property
     def fallback(self) -> dict[str, int]:

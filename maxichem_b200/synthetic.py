@@ -343,6 +343,8 @@ def workload(net: VulcanNetwork, kind: str, cells: int, seed: int = 0) -> Worklo
 
     kind "cfg0": T log-uniform 500-2500 K, P log-uniform 1e-2..1e8, solar start, h 1e-8 s, dt 1e10 s, dark.
     kind "column": the column grid (64 levels), solar start, h 1e-8 s, dt 300 s, upper-layer J.
+    kind "uneven": the column grid with the second half of the columns at night (J = 0); ``cold_start`` then turns a
+    quarter of the cells of settled states into cold starts.
     """
     rng = np.random.default_rng(seed)
     nj = len(net.photo)
@@ -358,6 +360,27 @@ def workload(net: VulcanNetwork, kind: str, cells: int, seed: int = 0) -> Worklo
         T, P = T[:cells], P[:cells]
         dt = np.full(cells, 300.0)
         J = photolysis_rates(P, nj, rng)
+    elif kind == "uneven":
+        levels = 64
+        columns = -(-cells // levels)
+        T, P = column_grid(levels, columns, rng)
+        T, P = T[:cells], P[:cells]
+        dt = np.full(cells, 300.0)
+        J = photolysis_rates(P, nj, rng)
+        J[np.arange(cells) // levels >= columns // 2] = 0.0  # night side
     else:
         raise ValueError(f"unknown workload kind {kind}")
     return Workload(solar_state(net, cells), T, P, dt, np.full(cells, 1e-8), J)
+
+
+def cold_start(x: np.ndarray, h: np.ndarray, seed: int = 0, share: float = 0.25, sigma: float = 2.0):
+    """A copy of settled states in which every cell of a seeded `share` is a cold start: x multiplied by a log-normal
+    factor of width sigma per species and renormalised, h 1e-10 s. Returns x, h and the cold cells' mask."""
+    rng = np.random.default_rng(seed)
+    x, h = np.array(x, dtype=np.float64), np.array(h, dtype=np.float64)
+    cold = rng.random(x.shape[0]) < share
+    f = np.exp(sigma * rng.standard_normal((int(cold.sum()), x.shape[1])))
+    xc = x[cold] * f
+    x[cold] = xc / xc.sum(1, keepdims=True)
+    h[cold] = 1e-10
+    return x, h, cold

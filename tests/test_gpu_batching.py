@@ -1,0 +1,86 @@
+"""Batching forms on the GPU: every grid choice (persistent CTAs per SM, or one CTA per cell) gives the same bits, the
+autotuner picks one of them and leaves the counts alone, and a call loop captured in a CUDA graph gives the same
+results and counts as the same calls made one by one."""
+
+import numpy as np
+import pytest
+import torch
+
+from maxichem_b200 import autotune, graph, synthetic
+from maxichem_b200.solver import CudaSolver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def uneven(gpu, networks):
+    net = networks("cho41")
+    w = synthetic.workload(net, "uneven", 1024, seed=4)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=gpu)
+    solver = CudaSolver(net, gpu, photo=True)
+    x, h, _, _ = solver(t(w.x), t(w.T), t(w.P), t(w.dt), t(w.h), J=t(w.J))
+    xc, hc, cold = synthetic.cold_start(x.cpu().numpy(), h.cpu().numpy(), seed=5)
+    yield solver, (t(xc), t(w.T), t(w.P), t(w.dt), t(hc), t(w.J)), cold
+    solver.close()
+
+
+def call(solver, args):
+    x, T, P, dt, h, J = args
+    return solver.launch(x, T, P, dt, h, J=J)
+
+
+def test_every_grid_gives_the_same_bits(uneven):
+    solver, args, cold = uneven
+    solver.set_grid(-1)
+    ref = call(solver, args)
+    assert solver.info["grid_ctas_per_sm"] == solver.info["call_ctas_per_sm"]
+    for grid in (0, 1, solver.info["call_ctas_per_sm"]):
+        solver.set_grid(grid)
+        assert solver.info["grid_ctas_per_sm"] == grid
+        got = call(solver, args)
+        assert all(torch.equal(a, b) for a, b in zip(got, ref, strict=True)), grid
+    solver.set_grid(-1)
+    steps = ref.steps.cpu().numpy()
+    assert steps[cold].mean() > 3 * steps[~cold].mean()  # the batch is uneven
+
+
+def test_a_grid_beyond_the_occupancy_limit_is_refused(uneven):
+    solver, _, _ = uneven
+    with pytest.raises(ValueError, match="ctas_per_sm from -1 to"):
+        solver.set_grid(solver.info["call_ctas_per_sm"] + 1)
+    with pytest.raises(ValueError, match="ctas_per_sm from -1 to"):
+        solver.set_grid(-2)
+
+
+def test_the_tuner_picks_a_grid_and_keeps_the_counts(uneven):
+    solver, (x, T, P, dt, h, J), _ = uneven
+    before = solver.total.clone()
+    got = autotune.tune_grid(solver, x, T, P, dt, h, J=J, choices=[0, 1, solver.info["call_ctas_per_sm"]])
+    assert got["best"] in (0, 1, solver.info["call_ctas_per_sm"])
+    assert set(got["ms"]) == {0, 1, solver.info["call_ctas_per_sm"]} and all(v > 0 for v in got["ms"].values())
+    assert solver.info["grid_ctas_per_sm"] == got["best"]
+    assert autotune.cached(solver, x.shape[0]) == got["best"]
+    assert torch.equal(solver.total, before)
+    solver.set_grid(-1)
+
+
+def test_a_captured_loop_equals_the_calls_one_by_one(uneven):
+    solver, (x, T, P, dt, h, J), _ = uneven
+    calls = 3
+    before = solver.total.clone()
+    xs, hs, outs = x, h, []
+    for _ in range(calls):
+        r = solver.launch_raw(xs, T, P, dt, hs, rtol=1e-3, atol=1e-25, max_steps=4000, J=J)
+        outs.append({k: v.clone() for k, v in r.items()})
+        xs, hs = r["x"], r["h"]
+    eager_total = solver.total - before
+    loop = graph.CallLoop(solver, x, T, P, dt, h, J=J, calls=calls)
+    mid = solver.total.clone()
+    last = loop.run()
+    torch.cuda.synchronize()
+    for k in ("x", "h", "steps", "done", "flag", "status"):
+        assert torch.equal(last[k], outs[-1][k]), k
+    assert torch.equal(solver.total - mid, eager_total)
+    loop.carry()
+    assert torch.equal(loop.x_in, outs[-1]["x"]) and torch.equal(loop.h_in, outs[-1]["h"])
+    loop.close()
