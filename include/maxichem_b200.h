@@ -200,6 +200,12 @@ int mx_time_phases(mx_solver* s, const double* x, double T, double P, double h, 
  * file does not hold. */
 int mx_probe_fp64(int device, int64_t iters, double* gflops);
 
+/* A solver from a folder that CudaSolver.export wrote (meta.txt and tables/<name>.bin: the network's tables and the
+ * drift allowance), for a caller without Python; replaces the reference's export loader (cpp/maxichem.cpp:40-171).
+ * The folder is read and checked completely before any CUDA work: a missing or malformed table returns
+ * MX_ERR_NETWORK. */
+int mx_create_from_export(const char* folder, int device, mx_solver** out, char* err, size_t errlen);
+
 /* Release the solver's device memory. Safe on NULL. */
 int mx_destroy(mx_solver* s);
 

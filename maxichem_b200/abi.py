@@ -101,6 +101,7 @@ _ERR = ctypes.c_char_p
 # Every entry point that include/maxichem_b200.h declares, with its ctypes signature.
 SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "mx_create": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_P), _ERR, ctypes.c_size_t]),
+    "mx_create_from_export": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_P), _ERR, ctypes.c_size_t]),
     "mx_call": (
         ctypes.c_int,
         [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_int32,

@@ -11,6 +11,7 @@ from __future__ import annotations
 import ctypes
 import math
 import operator
+from pathlib import Path
 from typing import Any, NamedTuple
 
 import numpy as np
@@ -133,6 +134,7 @@ class CudaSolver:
         if not (math.isfinite(value) and value >= 0.0):
             raise ValueError(f"drift: a finite allowance of at least 0 expected, got {drift}")
         self.drift = value
+        self.net = net
         self.dev = _device_of(device)
         self.tab = tables.build(net, photo)
         self.ns, self.nr, self.nj = self.tab.ns, self.tab.nr, self.tab.nj
@@ -225,6 +227,16 @@ class CudaSolver:
         """Advance each cell by dt: ``launch`` without the flag in its result (``self.flag`` keeps it)."""
         r = self.launch(x, T, P, dt, h, rtol=rtol, atol=atol, max_steps=max_steps, J=J)
         return CallResult(r.x, r.h, r.done, r.steps)
+
+    def export(self, folder: str | Path) -> Path:
+        """Write what a caller without Python needs to build this solver (include/maxichem_b200.hpp and
+        mx_create_from_export load it): meta.txt and tables/<name>.bin, the network's tables, names and the drift
+        allowance (kincuda.py:363-373). The kernels are the library's own, so no kernel code is written."""
+        self._require_open()
+        from .export import write_export
+
+        return write_export(self.tab, folder, drift=self.drift, species=list(self.net.species),
+                            elements=list(self.net.elements))  # fmt: skip
 
     def set_grid(self, ctas_per_sm: int) -> None:
         """The call kernel's grid for later calls: 1 .. info["call_ctas_per_sm"] persistent CTAs per SM over the cell
