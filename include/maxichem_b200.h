@@ -206,6 +206,19 @@ int mx_probe_fp64(int device, int64_t iters, double* gflops);
  * MX_ERR_NETWORK. */
 int mx_create_from_export(const char* folder, int device, mx_solver** out, char* err, size_t errlen);
 
+/* The GCM step's conversions either side of a call (replace maxichem/coupling/composition.py:102-183), on device
+ * arrays of B cells, asynchronous on stream; one pass over [B][ns] each, one warp per cell, row sums in the warp's
+ * order (lane l adds entries l, l + 32, ..., then a butterfly).
+ * mx_mass_to_mole: mass mixing ratios q -> mole fractions x = (q / mw) / sum(q / mw). *bad (device int32, zeroed by
+ * the call) gets bit 1 for a non-finite q, and unless signed_ok bit 2 for a negative q and bit 4 for a cell whose
+ * sum is not above 0. With signed_ok (signed_mole_fractions, composition.py:130-151) negatives pass through.
+ * mx_mole_to_mass: x and each cell's tracer mass -> q = x mw (mass / sum(x mw)); *bad gets bit 1 for a non-finite x,
+ * 2 for a negative x, 4 for a cell whose sum of x mw is not above 0, 8 for a mass negative or not finite. */
+int mx_mass_to_mole(const double* q, const double* mw, int64_t B, int32_t ns, int32_t signed_ok, double* x,
+                    int32_t* bad, void* stream);
+int mx_mole_to_mass(const double* x, const double* mw, const double* mass, int64_t B, int32_t ns, double* q,
+                    int32_t* bad, void* stream);
+
 /* Release the solver's device memory. Safe on NULL. */
 int mx_destroy(mx_solver* s);
 

@@ -118,6 +118,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     ),
     "mx_info": (ctypes.c_int, [_P, _P, ctypes.c_int32]),
     "mx_set_grid": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "mx_mass_to_mole": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P, _P, _P]),
+    "mx_mole_to_mass": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, ctypes.c_int32, _P, _P, _P]),
     "mx_destroy": (ctypes.c_int, [_P]),
     "mx_set_try_counter": (ctypes.c_int, [_P, _P]),
     "mx_set_phase_counter": (ctypes.c_int, [_P, _P]),
