@@ -277,29 +277,29 @@ __device__ __forceinline__ void jacobian_w(const Net& net, const Cell& c, double
   __syncthreads();
 }
 
-// ---- dense LU without exchanges, blocked (PANEL pivots at a time) ----
+// ---- dense LU without exchanges, blocked (PANEL pivots at a time), with a lookahead of one panel ----
 // Every entry receives its updates A_ij <- fma(-l_ik, A_kj, A_ij) in ascending k, l_ik = A_ik / A_kk taken as
 // A_ik * (1 / A_kk): the order and the operations of the right-looking LU, so the bits of the sparse factorisation
-// on the fill pattern (call.cuh:81-112) for finite data. Per block: the panel's pivots one by one (one thread per
-// row), the block's pivot rows beyond the panel (one thread per column), then the trailing matrix as a rank-PANEL
-// update in 4 x 4 register tiles spread over the CTA (rows and columns cyclic, so a warp's loads are broadcast or
-// consecutive).
+// on the fill pattern (call.cuh:81-112) for finite data. Per block: the block's pivot rows beyond the panel (one
+// thread per column); then warp 0 applies the block to the next panel's columns and factors that panel (one lane per
+// row, warp syncs only) while warps 1-3 apply it to the columns past the next panel, as a rank-PANEL update in 4 x 4
+// register tiles (rows and columns cyclic, so a warp's loads are broadcast or consecutive).
 
-// The trailing rows and columns [ke, ns) less L[:, kb..kb+nb) U[kb..kb+nb, :], tiles of 4 x 4 per thread.
+// the trailing update of rows ke.. and columns cs.. (cs >= ke) by NT threads
 template <int NT>
-__device__ __forceinline__ void trailing_update(double* A, int ld, int kb, int nb, int ke, int ns, int tid) {
-  constexpr int CG = 16, RG = NT / CG;  // column groups x row groups
-  const int cg = tid % CG, rg = tid / CG, m = ns - ke;
-  for (int rb = rg; rb < m; rb += 4 * RG) {    // the tile's rows: ke + rb + RG a, a < 4
-    for (int cb = cg; cb < m; cb += 4 * CG) {  // its columns: ke + cb + CG b, b < 4
+__device__ __forceinline__ void trailing_update_from(double* A, int ld, int kb, int nb, int ke, int cs, int ns, int tid) {
+  constexpr int CG = 16, RG = NT / CG;
+  const int cg = tid % CG, rg = tid / CG, m = ns - ke, mc = ns - cs;
+  for (int rb = rg; rb < m; rb += 4 * RG) {
+    for (int cb = cg; cb < mc; cb += 4 * CG) {
       int row[4], col[4];
       bool rok[4], cok[4];
 #pragma unroll
       for (int a = 0; a < 4; a++) {
         rok[a] = rb + RG * a < m;
         row[a] = ke + (rok[a] ? rb + RG * a : 0);
-        cok[a] = cb + CG * a < m;
-        col[a] = ke + (cok[a] ? cb + CG * a : 0);
+        cok[a] = cb + CG * a < mc;
+        col[a] = cs + (cok[a] ? cb + CG * a : 0);
       }
       double acc[4][4];
 #pragma unroll
@@ -330,32 +330,40 @@ __device__ __forceinline__ void trailing_update(double* A, int ld, int kb, int n
   }
 }
 
+// the panel kb .. kb + nb - 1 on one warp (lane), warp-level syncs only
+__device__ __forceinline__ void panel_warp(double* A, int ld, double* dinv, int kb, int nb, int ns, int lane) {
+  const int ke = kb + nb;
+  if (lane == 0) dinv[kb] = __drcp_rn(A[kb * ld + kb]);
+  __syncwarp();
+  for (int k = kb; k < ke; k++) {
+    const double d = dinv[k];
+    double piv[PANEL];
+#pragma unroll
+    for (int jj = 1; jj < PANEL; jj++) piv[jj] = k + jj < ke ? A[k * ld + k + jj] : 0.0;
+    for (int i = k + 1 + lane; i < ns; i += 32) {
+      double* ai = A + i * ld;
+      const double l = ai[k] * d;
+      ai[k] = l;
+#pragma unroll
+      for (int jj = 1; jj < PANEL; jj++)
+        if (k + jj < ke) ai[k + jj] = fma(-l, piv[jj], ai[k + jj]);
+      if (i == k + 1 && i < ke) dinv[i] = __drcp_rn(ai[i]);
+    }
+    __syncwarp();
+  }
+}
+
+// the blocked LU with a lookahead of one panel: while warps 1-3 apply panel p to the columns past panel p + 1, warp 0
+// applies it to panel p + 1's columns and factors panel p + 1. Each entry takes its updates in ascending pivot order.
 template <int NT>
 __device__ __forceinline__ void lu_factor(const Net& net, double* A, double* dinv, int tid) {
-  const int ns = net.ns, ld = net.ld;
+  const int ns = net.ns, ld = net.ld, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) panel_warp(A, ld, dinv, 0, min(PANEL, ns), ns, lane);
+  __syncthreads();
   for (int kb = 0; kb < ns; kb += PANEL) {
     const int ke = min(kb + PANEL, ns), nb = ke - kb;
-    if (tid == 0) dinv[kb] = __drcp_rn(A[kb * ld + kb]);  // 1 / x, correctly rounded: the bits of 1.0 / x
-    __syncthreads();
-    for (int k = kb; k < ke; k++) {  // the panel: columns kb..ke-1
-      const double d = dinv[k];
-      double piv[PANEL];
-#pragma unroll
-      for (int jj = 1; jj < PANEL; jj++) piv[jj] = k + jj < ke ? A[k * ld + k + jj] : 0.0;
-      for (int i = k + 1 + tid; i < ns; i += NT) {
-        double* ai = A + i * ld;
-        const double l = ai[k] * d;
-        ai[k] = l;
-#pragma unroll
-        for (int jj = 1; jj < PANEL; jj++)
-          if (k + jj < ke) ai[k + jj] = fma(-l, piv[jj], ai[k + jj]);
-        if (i == k + 1 && i < ke) dinv[i] = __drcp_rn(ai[i]);  // the next pivot, final now
-      }
-      __syncthreads();
-    }
     if (ke == ns) break;
-    // the block's pivot rows beyond the panel: row kb + s takes pivots kb .. kb + s - 1
-    for (int j = ke + tid; j < ns; j += NT) {
+    for (int j = ke + tid; j < ns; j += NT) {  // the block's pivot rows beyond the panel
       double row[PANEL];
 #pragma unroll
       for (int s = 0; s < PANEL; s++) row[s] = s < nb ? A[(kb + s) * ld + j] : 0.0;
@@ -372,7 +380,26 @@ __device__ __forceinline__ void lu_factor(const Net& net, double* A, double* din
       }
     }
     __syncthreads();
-    trailing_update<NT>(A, ld, kb, nb, ke, ns, tid);
+    const int ken = min(ke + PANEL, ns);
+    if (warp == 0) {
+      for (int i = ke + lane; i < ns; i += 32) {  // panel p + 1's columns, rows ke..
+        double* ai = A + i * ld;
+        double l[PANEL];
+#pragma unroll
+        for (int t = 0; t < PANEL; t++) l[t] = t < nb ? ai[kb + t] : 0.0;
+        for (int j = ke; j < ken; j++) {
+          double acc = ai[j];
+#pragma unroll
+          for (int t = 0; t < PANEL; t++)
+            if (t < nb) acc = fma(-l[t], A[(kb + t) * ld + j], acc);
+          ai[j] = acc;
+        }
+      }
+      __syncwarp();
+      panel_warp(A, ld, dinv, ke, ken - ke, ns, lane);
+    } else {
+      trailing_update_from<NT - 32>(A, ld, kb, nb, ke, ken, ns, tid - 32);
+    }
     __syncthreads();
   }
 }

@@ -110,10 +110,15 @@ __global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const Ca
       mark(PH_RHS_JAC);
       lu_factor<32 * W>(net, c.A, c.dinv, tid);
       mark(PH_LU);
-      if (warp == 0) {  // stage 1: K1 and M0^-1 w together, then Sherman-Morrison
+      if (warp == 0) {  // stage 1: K1 on warp 0 and M0^-1 w on warp 1 (msolve, call.cuh:122-131), then Sherman-Morrison
         for (int i = lane; i < ns; i += 32) c.K1[i] = c.F[i];
         __syncwarp();
-        lu_solve<R, 2>(net, c.A, c.dinv, c.K1, c.U, lane);
+        lu_solve<R, 1>(net, c.A, c.dinv, c.K1, nullptr, lane);
+      } else if (warp == 1) {
+        lu_solve<R, 1>(net, c.A, c.dinv, c.U, nullptr, lane);
+      }
+      __syncthreads();
+      if (warp == 0) {
         c0 = 1.0 / (1.0 - lane_sum(c.U, ns, lane));
         sherman(net, c.K1, c.U, c0, lane);
       }
