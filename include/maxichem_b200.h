@@ -225,6 +225,10 @@ int mx_destroy(mx_solver* s);
 /* The library's build identity (architecture and version), a static string. */
 const char* mx_version(void);
 
+/* Warps per cell of the call kernel: mx_network's stream groups must have 32 x that and 32 x (that - 1) threads
+ * (maxichem_b200/tables.py stream_groups). No counterpart in the reference. */
+int mx_warps_per_cell(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,7 +79,7 @@ class NetworkStruct:
         piece, row_ptr = tables.sv_row_pieces(tab)
         self.struct.sv_piece, self.struct.n_pieces = piece, int(row_ptr[-1])
         self.struct.sv_row_ptr = ptr(row_ptr, np.int32)
-        for g, threads in enumerate((128, 96)):
+        for g, threads in enumerate(tab.stream_groups):
             st = tab.streams.get(threads)
             if st is None:
                 continue
@@ -133,6 +133,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     ),
     "mx_probe_fp64": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
     "mx_version": (ctypes.c_char_p, []),
+    "mx_warps_per_cell": (ctypes.c_int, []),
 }
 
 _lib: ctypes.CDLL | None = None

@@ -1063,3 +1063,5 @@ extern "C" int mx_call_static(mx_solver* s, const double* x, const double* T, co
 }
 
 extern "C" const char* mx_version(void) { return "maxichem_b200 0.1 sm_100a"; }
+
+extern "C" int mx_warps_per_cell(void) { return WARPS; }

@@ -48,7 +48,7 @@ def write_export(tab: tables.Tables, folder: str | Path, *, drift: float, specie
     for name, dtype in _ARRAYS:
         table(name, getattr(tab, name), dtype)
     table("sv_row_ptr", row_ptr, np.int32)
-    for g, threads in enumerate((128, 96)):
+    for g, threads in enumerate(tab.stream_groups):
         st = tab.streams[threads]
         lines.append(f"group {g} {threads} {st['sv'].shape[0]} {st['sv_rows'].shape[0]} {st['jt'].shape[0]} "
                      f"{st['jac_dst'].shape[0]}")  # fmt: skip

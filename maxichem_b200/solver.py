@@ -136,12 +136,12 @@ class CudaSolver:
         self.drift = value
         self.net = net
         self.dev = _device_of(device)
-        self.tab = tables.build(net, photo)
+        self._lib = abi.library()
+        self.tab = tables.build(net, photo, warps=int(self._lib.mx_warps_per_cell()))
         self.ns, self.nr, self.nj = self.tab.ns, self.tab.nr, self.tab.nj
         self.count = torch.zeros(abi.COUNT_SLOTS, dtype=torch.int32, device=self.dev)
         self.total = torch.zeros(abi.COUNT_SLOTS, dtype=torch.int64, device=self.dev)
         self.flag: torch.Tensor | None = None
-        self._lib = abi.library()
         struct = abi.NetworkStruct(self.tab)
         handle = ctypes.c_void_p()
         err = ctypes.create_string_buffer(_ERRLEN)

@@ -131,6 +131,7 @@ class Tables:
     has_eff: bool
     flops: dict[str, float] = field(default_factory=dict)
     streams: dict[int, dict[str, np.ndarray]] = field(default_factory=dict)  # per-thread term streams by group size
+    stream_groups: tuple[int, int] = (128, 96)  # the group sizes of the call kernel, CTA first
     species: list[str] = field(default_factory=list)
     elements: list[str] = field(default_factory=list)
     photo: bool = False
@@ -139,8 +140,10 @@ class Tables:
 _CODE = {1.0: 0, -1.0: 1, 2.0: 2, -2.0: 3}
 
 
-def build(net: VulcanNetwork, photo: bool) -> Tables:
-    """Build the tables of ``net``; with ``photo`` its photolysis branches follow the thermal reactions."""
+def build(net: VulcanNetwork, photo: bool, warps: int = 4) -> Tables:
+    """Build the tables of ``net``; with ``photo`` its photolysis branches follow the thermal reactions. ``warps``:
+    the call kernel's warps per cell, which sets the thread groups of the term streams (the sums do not depend on
+    it)."""
     reactions = net.reac + (net.photo if photo else [])
     S = np.asarray(net.S, np.float64)
     if photo:
@@ -235,12 +238,19 @@ def build(net: VulcanNetwork, photo: bool) -> Tables:
         species=list(net.species), elements=list(net.elements), photo=photo,
     )  # fmt: skip
     tab.flops = work_counts(tab)
-    for threads in STREAM_GROUPS:
+    tab.stream_groups = stream_groups(warps)
+    for threads in tab.stream_groups:
         tab.streams[threads] = thread_streams(tab, threads)
     return tab
 
 
-STREAM_GROUPS = (128, 96)  # the call kernel's CTA, and its warps 1-3 (which evaluate F(Y3) during stage 2)
+def stream_groups(warps: int) -> tuple[int, int]:
+    """The thread groups the call kernel streams sums over: its CTA of `warps` warps, and the warps past the first
+    (which evaluate F(Y3) while warp 0 solves stage 2)."""
+    return (32 * warps, 32 * (warps - 1))
+
+
+STREAM_GROUPS = stream_groups(4)  # the library's default CTA of 4 warps
 SV_END = 1 << 13
 J_END = 1 << 14
 

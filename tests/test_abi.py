@@ -83,5 +83,6 @@ def test_a_network_struct_points_at_its_tables(networks, name):
     s = abi.NetworkStruct(tab)
     st = s.struct
     assert (st.ns, st.nr, st.nj, st.nel) == (tab.ns, tab.nr, tab.nj, tab.atoms.shape[1])
-    assert list(st.stream_threads) == [128, 96]
+    assert list(st.stream_threads) == list(tab.stream_groups) == [128, 96]
+    assert abi.library().mx_warps_per_cell() == 4
     assert all(p for p in (st.perm, st.rx, st.rc, st.rf, st.nasa, st.atoms, st.sv_row_ptr))
