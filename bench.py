@@ -52,6 +52,9 @@ def parse() -> argparse.Namespace:
     p.add_argument("--workload", choices=("column", "uneven"), default="column",
                    help="uneven: 262,144 cells, half at night, a quarter cold starts, a loop of --calls calls")
     p.add_argument("--calls", type=int, default=100, help="calls of the uneven workload's loop")
+    p.add_argument("--network", choices=("cho41", "chno69", "sncho91"), default=NETWORK,
+                   help="the synthetic network (the metric is quoted on chno69)")
+    p.add_argument("--dt", type=float, default=DT, help="the call's dt, s (300; the sulfur configuration uses 600)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -164,9 +167,10 @@ def main() -> None:
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
-    net = synthetic.network(NETWORK)
+    net = synthetic.network(args.network)
     B = args.cells
     w = inputs(net, B, seed=replicas.seed(1000, rank))  # each rank its own batch of columns (weak scaling)
+    w.dt[:] = args.dt
     t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
     solver = CudaSolver(net, dev, photo=True)
     tab = solver.tab
@@ -219,10 +223,13 @@ def main() -> None:
     # the call's HBM I/O: x, T, P, dt, h, J in; x, h, steps (f64) and done, flag, status (int32) out
     io_bytes = B * (8 * (2 * tab.ns + tab.nj + 6) + 12)
     line = {
-        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC if (args.network, args.dt) == (NETWORK, DT) else
+                  f"cells/s per GCM call ({tab.ns}-sp, {B * world} cells, dt {args.dt:g} s): FP64 Rodas3",
+        "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded 69-species network and column grid; the VULCAN networks are absent)",
-        "config": {"workload": f"{NETWORK}: call {SPINUP_CALLS + 1} of 300 s calls on a {LEVELS}-level column grid",
+        "config": {"workload": f"{args.network}: call {SPINUP_CALLS + 1} of {args.dt:g} s calls on a {LEVELS}-level "
+                               "column grid",
                    "cells_per_gpu": B, "species": tab.ns, "reactions": tab.nr, "photolysis": tab.nj,
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
                    "accepted_steps_mean": steps_mean, "tries_per_cell": nt[0] / args.steps / B,
