@@ -347,8 +347,10 @@ __device__ __forceinline__ void panel_warp(double* A, int ld, double* dinv, int 
 #pragma unroll
       for (int jj = 1; jj < PANEL; jj++)
         if (k + jj < ke) ai[k + jj] = fma(-l, piv[jj], ai[k + jj]);
-      if (i == k + 1 && i < ke) dinv[i] = __drcp_rn(ai[i]);
     }
+    // the next pivot is final now and its row is lane 0's (its first row), so lane 0 takes the reciprocal of its own
+    // write, after the row loop
+    if (lane == 0 && k + 1 < ke) dinv[k + 1] = __drcp_rn(A[(k + 1) * ld + k + 1]);
     __syncwarp();
   }
 }
