@@ -359,7 +359,8 @@ def ctypes_probe(lib, device: int) -> float:
 
 
 def e2e(solver, x, h, w, dev, args) -> dict:
-    """The same call through the public API from pinned host buffers: H2D, call (with its count read-back), D2H."""
+    """The same call through the public API from pinned host buffers (CudaSolver.call_host): H2D, the call with its
+    count read-back, D2H, overlapped over four pieces of the batch."""
     import torch
 
     pin = lambda a: torch.as_tensor(a, dtype=torch.float64).pin_memory()
@@ -368,13 +369,11 @@ def e2e(solver, x, h, w, dev, args) -> dict:
     odone = torch.empty(hh.shape, dtype=torch.bool).pin_memory()
     stream = torch.cuda.current_stream(dev)
 
-    def step():
-        d = [a.to(dev, non_blocking=True) for a in (hx, hT, hP, hdt, hh, hJ)]
-        r = solver(d[0], d[1], d[2], d[3], d[4], J=d[5])
-        ox.copy_(r.x, non_blocking=True)
-        oh.copy_(r.h, non_blocking=True)
-        odone.copy_(r.done, non_blocking=True)
-        ost.copy_(r.steps, non_blocking=True)
+    oflag, ostatus = (torch.empty(hh.shape, dtype=torch.int32).pin_memory() for _ in range(2))
+    out = {"x": ox, "h": oh, "steps": ost, "done": odone, "flag": oflag, "status": ostatus}
+
+    def step():  # the call on host buffers: copies in, kernels and copies out overlapped over pieces of the batch
+        solver.call_host(hx, hT, hP, hdt, hh, J=hJ, out=out)
 
     for _ in range(max(1, args.warmup)):
         step()
@@ -387,7 +386,7 @@ def e2e(solver, x, h, w, dev, args) -> dict:
     torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1) / args.steps
     h2d = sum(a.numel() * a.element_size() for a in (hx, hT, hP, hdt, hh, hJ))
-    d2h = sum(a.numel() * a.element_size() for a in (ox, oh, odone, ost))
+    d2h = sum(a.numel() * a.element_size() for a in (ox, oh, odone, ost, oflag, ostatus))
     return {"value": hx.shape[0] / (ms * 1e-3), "unit": "cells/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms}  # fmt: skip
 

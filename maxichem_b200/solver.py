@@ -250,6 +250,60 @@ class CudaSolver:
         self._lib.mx_info(self._handle, values, len(INFO_FIELDS))
         self.info["grid_ctas_per_sm"] = int(values[len(INFO_FIELDS) - 1])
 
+    def call_host(self, x: torch.Tensor, T: torch.Tensor, P: torch.Tensor, dt: torch.Tensor, h: torch.Tensor, *,
+                  rtol: float = DEFAULT_RTOL, atol: float = ATOL, max_steps: int = DEFAULT_MAX_STEPS,
+                  J: torch.Tensor | None = None, chunks: int = 4,
+                  out: dict[str, torch.Tensor] | None = None) -> CallResult:
+        """The call on host (CPU) tensors, with the copies overlapped: the batch goes in `chunks` pieces, each copied
+        in, solved and copied out on three streams, so piece k + 1 is copied in and piece k - 1 copied out while
+        piece k is solved (4 pieces measured best for 1M cells: more pieces add more kernel tails). Cells are independent, so the results, counts, flag and refusal are those of one call on
+        the whole batch. Pinned inputs overlap; `out` may hold pinned host outputs x, h, steps (float64), done (bool),
+        flag and status (int32) to write into (allocated, pinned, when None)."""
+        self._require_open()
+        self.flag = None
+        cpu = torch.device("cpu")
+        B = check_inputs(cpu, self.ns, x, T, P, dt, h, rtol, atol, max_steps)
+        jx = check_photolysis(J, B, self.nj, cpu)
+        if chunks < 1:
+            raise ValueError(f"chunks: at least 1 expected, got {chunks}")
+        if out is None:
+            f = lambda *shape, dtype=torch.float64: torch.empty(*shape, dtype=dtype).pin_memory()
+            out = {"x": f(B, self.ns), "h": f(B), "steps": f(B), "done": f(B, dtype=torch.bool),
+                   "flag": f(B, dtype=torch.int32), "status": f(B, dtype=torch.int32)}  # fmt: skip
+        ins = [a.contiguous() for a in (x, T, P, dt, h)] + ([jx] if jx is not None else [])
+        dev_in = [torch.empty(a.shape, dtype=a.dtype, device=self.dev) for a in ins]
+        dev_out = {
+            "x": torch.empty(B, self.ns, dtype=torch.float64, device=self.dev),
+            **{k: torch.empty(B, dtype=torch.float64, device=self.dev) for k in ("h", "steps")},
+            **{k: torch.empty(B, dtype=torch.int32, device=self.dev) for k in ("done", "flag", "status")},
+        }  # fmt: skip
+        main = torch.cuda.current_stream(self.dev)
+        s_in, s_run, s_out = (torch.cuda.Stream(self.dev) for _ in range(3))
+        for s in (s_in, s_run, s_out):
+            s.wait_stream(main)
+        before = self.total.clone()
+        step = -(-B // chunks) if B else 1
+        for a in range(0, B, step):
+            b = min(B, a + step)
+            with torch.cuda.stream(s_in):
+                for d, src in zip(dev_in, ins):
+                    d[a:b].copy_(src[a:b], non_blocking=True)
+            s_run.wait_stream(s_in)
+            with torch.cuda.stream(s_run):
+                sl = [d[a:b] for d in dev_in]
+                self.launch_raw(*sl[:5], J=sl[5] if jx is not None else None, rtol=rtol, atol=atol,
+                                max_steps=max_steps, out={k: v[a:b] for k, v in dev_out.items()})  # fmt: skip
+            s_out.wait_stream(s_run)
+            with torch.cuda.stream(s_out):
+                for k, v in dev_out.items():
+                    out[k][a:b].copy_(v[a:b], non_blocking=True)
+        main.wait_stream(s_out)
+        main.synchronize()
+        self.count.copy_((self.total - before).to(torch.int32))  # the counts of the whole call
+        self._refuse(*ins[:4], ins[5] if jx is not None else None, out["status"])
+        self.flag = out["flag"]
+        return CallResult(out["x"], out["h"], out["done"], out["steps"])
+
     @property
     def fallback(self) -> dict[str, int]:
         """The last call's counts (one small copy from the device)."""

@@ -381,3 +381,33 @@ def test_recovery_tries_ten_times_the_steps(case):
                  max_steps=3)  # fmt: skip
     assert r["flag"].tolist() == flag.tolist() and r["done"].tolist() == d.tolist()
     assert (n.cpu().numpy() <= 3 * REC_STEPS).all()
+
+
+@pytest.mark.parametrize("chunks", [1, 5])
+def test_the_host_call_is_the_device_call(case, chunks):
+    # the call on host tensors, copies overlapped over pieces of the batch, gives the device call's bits and counts
+    s = case.solver
+    args = (case.xs, case.T, case.P, case.full(300.0), case.hs)
+    ref = s.launch(*args, J=case.J)
+    ref_count, ref_flag = s.count.clone(), ref.flag.clone()
+    before = s.total.clone()
+    pin = lambda a: a.cpu().pin_memory()
+    got = s.call_host(*(pin(a) for a in args), J=pin(case.J), chunks=chunks)
+    assert all(torch.equal(a.cpu(), b) for a, b in zip(ref[:4], got, strict=True))
+    assert torch.equal(s.count, ref_count) and torch.equal(s.flag, ref_flag.cpu())
+    assert torch.equal(s.total - before, ref_count.to(torch.int64))
+
+
+def test_the_host_call_refuses_like_the_device_call(case):
+    s = case.solver
+    x = case.xs.cpu().clone()
+    x[6, 2] = float("nan")
+    T = case.T.cpu().clone()
+    T[9] = 250.0
+    with pytest.raises(ValueError, match=r"1 cells below 300 K, .*\(first: cell 9, T = 250 K\).*1 cells of bad input: .*"
+                                         r"\(first: cell 6: sum\(x\) - 1 = nan"):
+        s.call_host(x, T, case.P.cpu(), case.full(1.0).cpu(), case.hs.cpu(), J=case.J.cpu(), chunks=3)
+    assert s.flag is None
+    with pytest.raises(ValueError, match=r"^T: float64"):
+        s.call_host(x, case.T, case.P.cpu(), case.full(1.0).cpu(), case.hs.cpu(), J=case.J.cpu())
+
