@@ -137,10 +137,13 @@ int mx_call(mx_solver* s, const double* x, const double* T, const double* P, con
 #define MX_STATIC_MAX_CELLS 1048576
 
 /*
- * mx_call for callers that cannot allocate device memory. No counterpart in the reference. Same arguments, results,
- * errors and kernels as mx_call, but the call's only scratch (the recompute list, one int32 per cell) is a file-scope
- * static device array of MX_STATIC_MAX_CELLS entries instead of solver-owned memory, so the call never calls
- * cudaMalloc, cudaFree or any allocating library routine (the solver handle itself still comes from mx_create).
+ * mx_call for callers that cannot allocate device memory. No counterpart in the reference. Such callers are, for
+ * instance, a GCM whose framework reserved the GPU's memory for its own pool at start-up (a cudaMalloc during the
+ * time loop then fails or fragments that pool), or a time loop that cannot afford the device-wide synchronisation
+ * that cudaMalloc and cudaFree may imply. Same arguments, results, errors and kernels as mx_call, but the call's
+ * only scratch (the recompute list, one int32 per cell) is a file-scope static device array of MX_STATIC_MAX_CELLS
+ * entries instead of solver-owned memory, so the call never calls cudaMalloc, cudaFree or any allocating library
+ * routine (the solver handle itself still comes from mx_create, once, at set-up).
  * - B above MX_STATIC_MAX_CELLS is refused with MX_ERR_ARGUMENT and a message naming the limit.
  * - The first call on a device looks up the array's address there (cudaGetSymbolAddress, with that device current)
  *   and keeps it; make that first call before any stream capture on the device.

@@ -969,7 +969,9 @@ extern "C" int mx_probe_fp64(int device, int64_t iters, double* gflops) {
 }
 
 // ---- mx_call_static: the call for callers that cannot allocate device memory ----
-// The only scratch a call owns is the recompute list (one int per cell). Here it is a file-scope device array of
+// For a GCM whose framework holds the GPU's memory in its own pool, or whose time loop must not pay the device-wide
+// synchronisation of cudaMalloc and cudaFree. The only scratch a call owns is the recompute list (one int per cell).
+// Here it is a file-scope device array of
 // MX_STATIC_MAX_CELLS entries that every mx_call_static call shares; its address on a device is looked up once, at
 // that device's first call, with the device current.
 

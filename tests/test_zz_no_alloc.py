@@ -1,6 +1,7 @@
-"""mx_call_static, the call that allocates nothing, against mx_call through the C-ABI: two calls in a row, the second
-from the first's results, give the same outputs and counts (collected last, and correct in a fresh process too: its
-first call on the device looks up the static scratch)."""
+"""mx_call_static, the call that allocates nothing (for a GCM whose framework keeps the GPU's memory in its own pool,
+or whose time loop must not pay cudaMalloc's synchronisation), against mx_call through the C-ABI: two calls in a row,
+the second from the first's results, give the same outputs and counts (collected last, and correct in a fresh
+process too: its first call on the device looks up the static scratch)."""
 
 import ctypes
 
