@@ -34,8 +34,8 @@ LEVELS = 64
 SPINUP_CALLS = 4
 DT = 300.0
 # DRAM bytes of one call-kernel launch per cell: ncu's dram__bytes_read.sum + dram__bytes_write.sum of the timed call
-# at 262,144 cells (412.69 MB), divided by its cells; a launch's traffic grows with its cells.
-TRAFFIC_PER_CELL = 412.69e6 / 262144
+# at 262,144 cells (411.78 MB), divided by its cells; a launch's traffic grows with its cells.
+TRAFFIC_PER_CELL = 411.78e6 / 262144
 HBM_GBS = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"] if (ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
 
 
