@@ -1,4 +1,5 @@
-"""TEST INFRASTRUCTURE ONLY: the CPU oracle of the per-call chemistry solve (oracle/mx_oracle.c) through ctypes.
+"""TEST INFRASTRUCTURE ONLY: the CPU oracle of the per-call chemistry solve (oracle/mx_oracle.c) and of its tangent
+(oracle/mx_oracle_ad.c) through ctypes.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this package: as the checker of the CUDA
 path, or as the timed CPU baseline. The product (maxichem_b200) never imports it.
@@ -17,7 +18,7 @@ from maxichem_b200.abi import COUNT_SLOTS, NetworkStruct
 from maxichem_b200.tables import Tables
 
 HERE = Path(__file__).resolve().parent
-SOURCE = HERE / "mx_oracle.c"
+SOURCES = [HERE / "mx_oracle.c", HERE / "mx_oracle_ad.c"]
 LIBRARY = HERE / "_build" / "libmx_oracle.so"
 FLAGS = ["-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-std=c11", "-Wall"]
 
@@ -28,10 +29,11 @@ def build(force: bool = False) -> Path:
     """Compile the oracle with gcc (no contraction of multiply-adds: every fma is explicit)."""
     LIBRARY.parent.mkdir(exist_ok=True)
     header = HERE.parent / "include" / "maxichem_b200.h"
-    stale = not LIBRARY.exists() or max(SOURCE.stat().st_mtime, header.stat().st_mtime) > LIBRARY.stat().st_mtime
+    newest = max(p.stat().st_mtime for p in [*SOURCES, header])
+    stale = not LIBRARY.exists() or newest > LIBRARY.stat().st_mtime
     if force or stale:
         tmp = LIBRARY.with_suffix(".tmp.so")
-        subprocess.run(["gcc", *FLAGS, str(SOURCE), "-o", str(tmp), "-lm"], check=True)
+        subprocess.run(["gcc", *FLAGS, *map(str, SOURCES), "-o", str(tmp), "-lm"], check=True)
         tmp.replace(LIBRARY)
     return LIBRARY
 
@@ -57,6 +59,9 @@ def library() -> ctypes.CDLL:
         lib.mxo_screen.restype = ctypes.c_int
         lib.mxo_screen.argtypes = [P, P, D, D, D, P, P]
         lib.mxo_threads.restype = ctypes.c_int
+        lib.mxo_jvp.restype = ctypes.c_int
+        lib.mxo_jvp.argtypes = [P, D, P, P, P, P, P, P, P, P, I64, D, D, I32, I32, I32] + [P] * 8 + [P] * 9 + [
+            ctypes.c_int]
         lib.mxo_debug_try.restype = None
         lib.mxo_debug_try.argtypes = [P, P, D, D, D, P, D, D, P]
         _lib = lib
@@ -93,6 +98,39 @@ class Oracle:
                           max_steps, _p(xo), _p(ho), _p(done), _p(steps), _p(flag), _p(status), _p(count), threads)
         return {"x": xo, "h": ho, "done": done.astype(bool), "steps": steps, "flag": flag, "status": status,
                 "count": count}  # fmt: skip
+
+    def jvp(self, x: Any, T: Any, P: Any, dt: Any, h: Any, dx: Any = None, dT: Any = None, dP: Any = None,
+            ddt: Any = None, dh: Any = None, *, lm: Any = None, dlm: Any = None, rc: Any = None, drc: Any = None,
+            J: Any = None, dJ: Any = None, adapt: bool = True, rtol: float = 1e-3, atol: float = 1e-25,
+            max_steps: int = 4000, threads: int = 0) -> dict[str, np.ndarray]:
+        """One call and its tangent on the CPU (dual numbers through the oracle's call): the outputs of ``call`` and
+        dx [D, B, S], dh [D, B]. Every tangent has a leading axis of D directions (None: zeros; all None: D = 0, the
+        primal alone, which takes lm and rc as the tangent call does)."""
+        tab = self.tab
+        x, T, P, dt, h = (_f64(a) for a in (x, T, P, dt, h))
+        B, ns = x.shape
+        nr, nj = tab.nr, tab.nj
+        given = [a for a in (dx, dT, dP, ddt, dh, dlm, drc, dJ) if a is not None]
+        D = int(np.shape(given[0])[0]) if given else 0
+        z = lambda *s: np.zeros(s)
+        dx, dT, dP, ddt, dh = (_f64(a) if a is not None else z(D, *shape)
+                               for a, shape in ((dx, (B, ns)), (dT, (B,)), (dP, (B,)), (ddt, (B,)), (dh, (B,))))
+        opt = lambda a: None if a is None else _f64(a)
+        lm, dlm, rc, drc, dJ = (opt(a) for a in (lm, dlm, rc, drc, dJ))
+        Jc = _f64(J if J is not None and nj else np.zeros((B, nj)))
+        if dJ is not None and not nj:
+            dJ = None
+        xo, ho, steps = np.empty_like(x), np.empty(B), np.empty(B)
+        done, flag, status = (np.empty(B, np.int32) for _ in range(3))
+        count = np.zeros(COUNT_SLOTS, np.int32)
+        dxo, dho = np.empty((D, B, ns)), np.empty((D, B))
+        q = lambda a: None if a is None else _p(a)
+        self.lib.mxo_jvp(self.net.ref(), self.drift, _p(x), _p(T), _p(P), _p(dt), _p(h), _p(Jc), q(lm), q(rc), B, rtol,
+                         atol, max_steps, int(adapt), D, _p(dx), _p(dT), _p(dP), _p(ddt), _p(dh), q(dlm), q(drc), q(dJ),
+                         _p(xo), _p(ho), _p(done), _p(steps), _p(flag), _p(status), _p(count), _p(dxo), _p(dho),
+                         threads)  # fmt: skip
+        return {"x": xo, "h": ho, "done": done.astype(bool), "steps": steps, "flag": flag, "status": status,
+                "count": count, "dx": dxo, "dh": dho}  # fmt: skip
 
     def debug_try(self, x: Any, T: float, P: float, h: float, J: Any = None, rtol: float = 1e-3,
                   atol: float = 1e-25) -> dict[str, np.ndarray]:
