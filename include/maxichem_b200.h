@@ -157,6 +157,33 @@ int mx_call_static(mx_solver* s, const double* x, const double* T, const double*
                    double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag, int32_t* status,
                    int32_t* count, int64_t* total, void* stream, char* err, size_t errlen);
 
+/* Tangent directions of one mx_jvp call at most (the reference's DMAX, maxichem/_constants.py:29). */
+#define MX_JVP_MAX_DIRECTIONS 16
+
+/*
+ * One call and its tangent along D directions (replaces ADSolver.jvp's launches, maxichem/kincuda_ad.py:325-453):
+ * the call's screening, rates, Rodas3 steps, guard and recovery, with the derivative of x_out and h_out along each
+ * direction. The primal is mx_call's bit for bit when lm and rc are NULL.
+ * Inputs as mx_call's, and lm [B][nr] per-cell log rate multipliers (NULL: none; a multiplier scales both directions
+ * of a reaction after the collision limit, a photolysis branch has kf = J e^lm), rc [nr][14] the rate table (NULL:
+ * the network's). adapt: 1 differentiates the step control too (rejected tries included, h carried in and out), 0
+ * holds every accepted try's size fixed (no tangent through dt, h or the error; dh_out 0).
+ * Tangents, device arrays with a leading axis of D directions: dx [D][B][ns], dT, dP, ddt, dh [D][B], dlm [D][B][nr],
+ * drc [D][nr][9] (the nine Arrhenius columns), dJ [D][B][nj]; dlm, drc and dJ NULL for zero.
+ * Outputs as mx_call's, and dx_out [D][B][ns], dh_out [D][B]: the tangents of the result before the guard's
+ * element-share correction (conservation makes the correction's own sensitivity zero). A cell the guard recomputes
+ * is differentiated along the recovery's path; one that still fails (flag 2) has NaN tangents. A non-finite log
+ * multiplier is not a refusal: the cell takes no step and fails. Errors as mx_call's, and D outside
+ * 1..MX_JVP_MAX_DIRECTIONS or adapt not 0/1 (MX_ERR_ARGUMENT). Allocates the tangent kernels' scratch at the first
+ * call and when a call needs more. Calls run one at a time.
+ */
+int mx_jvp(mx_solver* s, const double* x, const double* T, const double* P, const double* dt, const double* h_in,
+           const double* J, const double* lm, const double* rc, int64_t B, double rtol, double atol, int32_t max_steps,
+           int32_t adapt, int32_t D, const double* dx, const double* dT, const double* dP, const double* ddt,
+           const double* dh, const double* dlm, const double* drc, const double* dJ, double* x_out, double* h_out,
+           int32_t* done, double* steps, int32_t* flag, int32_t* status, double* dx_out, double* dh_out,
+           int32_t* count, int64_t* total, void* stream, char* err, size_t errlen);
+
 /* The guard alone on given states (replaces a launch of the reference's guard kernel, maxichem/kernels/guard.cuh:114):
  * counts refused cells from status, checks and corrects the others in x_out, writes flag 0/1 and the recompute list
  * count. Device pointers; used by tests of the guard's thresholds. */

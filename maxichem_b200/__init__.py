@@ -7,7 +7,7 @@ solver module does, on first use.
 
 from .network import VulcanNetwork
 
-__all__ = ["CudaSolver", "CallResult", "LaunchResult", "VulcanNetwork"]
+__all__ = ["ADSolver", "CudaSolver", "CallResult", "JvpResult", "LaunchResult", "VulcanNetwork"]
 
 
 def __getattr__(name: str):
@@ -15,4 +15,8 @@ def __getattr__(name: str):
         from . import solver
 
         return getattr(solver, name)
+    if name in ("ADSolver", "JvpResult"):
+        from . import ad
+
+        return getattr(ad, name)
     raise AttributeError(name)

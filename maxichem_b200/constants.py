@@ -16,6 +16,11 @@ DEFAULT_RTOL = 1e-3
 DEFAULT_MAX_STEPS = 4000
 ATOL = 1e-25  # mole fraction
 
+# Derivative settings (maxichem/_constants.py:28-29).
+CAP = 100  # attempts a derivative call stores per cell before the adjoint checkpoints
+DMAX = 16  # tangent directions per jvp call (MX_JVP_MAX_DIRECTIONS)
+ARRHENIUS_COLUMNS = 9  # the rate table's differentiated columns: ln A, B, C of k0's two terms and of k_inf
+
 # Reader limit (maxichem/_constants.py:36): largest |G/RT(low) - G/RT(high)| at NASA_SPLIT_T.
 MAX_GIBBS_JUMP = 1.0e-5
 

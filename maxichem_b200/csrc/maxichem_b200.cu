@@ -582,6 +582,27 @@ struct DeviceScope {
 
 }  // namespace
 
+#include "jvp.cuh"
+
+namespace {
+
+typedef void (*JvpFn)(const Net, const CallArgs, const TanArgs, const TanLayout);
+typedef void (*JvpRecoverFn)(const Net, const CallArgs, const TanArgs, const TanLayout, int);
+
+// the tangent kernels for rows_per_lane R of the warp solves
+bool pick_jvp_kernels(int r, JvpFn* jvp, JvpRecoverFn* rec) {
+  switch (r) {
+    case 1: *jvp = jvp_kernel<WARPS, 1>; *rec = jvp_recover_kernel<WARPS, 1>; return true;
+    case 2: *jvp = jvp_kernel<WARPS, 2>; *rec = jvp_recover_kernel<WARPS, 2>; return true;
+    case 3: *jvp = jvp_kernel<WARPS, 3>; *rec = jvp_recover_kernel<WARPS, 3>; return true;
+    case 4: *jvp = jvp_kernel<WARPS, 4>; *rec = jvp_recover_kernel<WARPS, 4>; return true;
+    case 8: *jvp = jvp_kernel<WARPS, 8>; *rec = jvp_recover_kernel<WARPS, 8>; return true;
+    default: return false;
+  }
+}  // fmt: skip
+
+}  // namespace
+
 struct mx_solver {
   int device = 0;
   Net net{};
@@ -599,6 +620,14 @@ struct mx_solver {
   int64_t list_capacity = 0;
   unsigned long long* tries = nullptr;
   long long* phases = nullptr;
+  // the tangent kernels (set up at the first mx_jvp call)
+  JvpFn jvp = nullptr;
+  JvpRecoverFn jvp_recover = nullptr;
+  TanLayout tan_layout{};
+  size_t jvp_smem = 0;
+  int jvp_ctas = 0, jvp_recover_ctas = 0;
+  double* jvp_scratch = nullptr;
+  size_t jvp_scratch_doubles = 0;
 };
 
 namespace {
@@ -620,6 +649,9 @@ void release(mx_solver* s) {
   s->buffers.clear();
   if (s->list) cudaFree(s->list);
   s->list = nullptr;
+  if (s->jvp_scratch) cudaFree(s->jvp_scratch);
+  s->jvp_scratch = nullptr;
+  s->jvp_scratch_doubles = 0;
 }
 
 }  // namespace
@@ -1059,6 +1091,150 @@ extern "C" int mx_call_static(mx_solver* s, const double* x, const double* T, co
   }
   if (e != cudaSuccess) {
     set_error(err, errlen, "mx_call_static: %s", cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  return MX_OK;
+}
+
+// ---- mx_jvp: the call and its tangent ----
+
+namespace {
+
+// The tangent kernels' shared-memory layout and launch limits, once per solver.
+int setup_jvp(mx_solver* s, char* err, size_t errlen) {
+  if (s->jvp) return MX_OK;
+  const Net& net = s->net;
+  const int ns = net.ns, nr = net.nr;
+  TanLayout& l = s->tan_layout;
+  int off = net.doubles;
+  auto take = [&](int doubles) {
+    const int o = off;
+    off += (doubles + 1) & ~1;
+    return o;
+  };
+  l.stride = (ns + 2) & ~1;
+  l.oTN = take(ns + 1);
+  l.oTn = take(ns + 1);
+  l.oTF = take(ns + 1);
+  l.oTu = take(ns + 1);
+  l.oTY = take(ns + 1);
+  l.oJK = take(4 * l.stride);
+  l.oTK = take(4 * l.stride);
+  l.oZ = take(std::max(nr, ns) + 1);
+  l.doubles = off;
+  const size_t smem = (size_t)off * sizeof(double);
+  JvpFn jvp = nullptr;
+  JvpRecoverFn rec = nullptr;
+  if (!pick_jvp_kernels(s->rows_per_lane, &jvp, &rec)) {
+    set_error(err, errlen, "mx_jvp: no tangent kernels for %d rows per lane", s->rows_per_lane);
+    return MX_ERR_NETWORK;
+  }
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
+  if ((size_t)optin < smem) {
+    set_error(err, errlen, "the tangent kernels need %zu B of shared memory per cell; the device has %d per block",
+              smem, optin);
+    return MX_ERR_NETWORK;
+  }
+  cudaError_t e = cudaFuncSetAttribute((const void*)jvp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)rec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int a = 0, b = 0;
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (const void*)jvp, 32 * WARPS, smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)rec, 32 * WARPS, smem);
+  if (e == cudaSuccess && (a < 1 || b < 1)) e = cudaErrorInvalidConfiguration;
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_jvp: %s", cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  s->jvp_smem = smem;
+  s->jvp_ctas = a;
+  s->jvp_recover_ctas = b;
+  s->jvp = jvp;
+  s->jvp_recover = rec;
+  return MX_OK;
+}
+
+}  // namespace
+
+extern "C" int mx_jvp(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
+                      const double* h_in, const double* J, const double* lm, const double* rc, int64_t B, double rtol,
+                      double atol, int32_t max_steps, int32_t adapt, int32_t D, const double* dx, const double* dT,
+                      const double* dP, const double* ddt, const double* dh, const double* dlm, const double* drc,
+                      const double* dJ, double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag,
+                      int32_t* status, double* dx_out, double* dh_out, int32_t* count, int64_t* total, void* stream,
+                      char* err, size_t errlen) {
+  if (!s) {
+    set_error(err, errlen, "this solver was closed; build a new one");
+    return MX_ERR_CLOSED;
+  }
+  if (B < 0 || B > 0x7fffffff) {
+    set_error(err, errlen, "mx_jvp: B out of range: %lld", (long long)B);
+    return MX_ERR_ARGUMENT;
+  }
+  if (!(rtol > 0.0 && rtol < 1e300 && atol > 0.0 && atol < 1e300)) {
+    set_error(err, errlen, "rtol and atol finite and positive expected, got %g, %g", rtol, atol);
+    return MX_ERR_ARGUMENT;
+  }
+  if (max_steps < 1 || (int64_t)MX_REC_STEPS * max_steps > 0x7fffffff) {
+    set_error(err, errlen, "max_steps from 1 to %d expected, got %d", 0x7fffffff / MX_REC_STEPS, max_steps);
+    return MX_ERR_ARGUMENT;
+  }
+  if (D < 1 || D > MX_JVP_MAX_DIRECTIONS || (adapt != 0 && adapt != 1)) {
+    set_error(err, errlen, "mx_jvp: from 1 to %d directions and adapt 0 or 1 expected, got %d and %d",
+              MX_JVP_MAX_DIRECTIONS, D, adapt);
+    return MX_ERR_ARGUMENT;
+  }
+  if (!count || !total || (B > 0 && (!x || !T || !P || !dt || !h_in || !x_out || !h_out || !done || !steps ||
+                                     !flag || !status || (s->net.nj > 0 && !J) || !dx || !dT || !dP || !ddt ||
+                                     !dh || !dx_out || !dh_out))) {
+    set_error(err, errlen, "mx_jvp: a required array is null");
+    return MX_ERR_ARGUMENT;
+  }
+  DeviceScope scope(s->device);
+  if (scope.status != cudaSuccess) {
+    set_error(err, errlen, "mx_jvp: device %d: %s", s->device, cudaGetErrorString(scope.status));
+    return MX_ERR_CUDA;
+  }
+  int rcode = setup_jvp(s, err, errlen);
+  if (rcode) return rcode;
+  rcode = grow_list(s, std::max<int64_t>(B, 1), err, errlen);
+  if (rcode) return rcode;
+  const Net& n0 = s->net;
+  const long long slot = ((long long)D * (2 * n0.nr + 2 + n0.ns + 1 + 4) + 1) & ~1ll;
+  const int grid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)s->jvp_ctas * s->sms);
+  const int rgrid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)s->jvp_recover_ctas * s->sms);
+  const size_t need = (size_t)std::max(grid, rgrid) * (size_t)slot;
+  if (need > s->jvp_scratch_doubles) {
+    if (s->jvp_scratch) cudaFree(s->jvp_scratch);
+    s->jvp_scratch = nullptr;
+    s->jvp_scratch_doubles = 0;
+    const cudaError_t e = cudaMalloc(&s->jvp_scratch, need * sizeof(double));
+    if (e != cudaSuccess) {
+      set_error(err, errlen, "mx_jvp: the tangent scratch of %zu doubles: %s", need, cudaGetErrorString(e));
+      return MX_ERR_CUDA;
+    }
+    s->jvp_scratch_doubles = need;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
+  if (e == cudaSuccess && B > 0) {
+    Net net = s->net;
+    if (rc) net.rc = rc;  // the caller's rate table
+    const CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status,
+                     count, s->list, nullptr};
+    const TanArgs ta{lm, dx, dT, dP, ddt, dh, dlm, drc, s->net.nj > 0 ? dJ : nullptr, D, adapt, dx_out, dh_out,
+                     s->jvp_scratch, slot};
+    s->jvp<<<grid, 32 * WARPS, s->jvp_smem, st>>>(net, a, ta, s->tan_layout);
+    s->jvp_recover<<<rgrid, 32 * WARPS, s->jvp_smem, st>>>(net, a, ta, s->tan_layout, MX_REC_STEPS * max_steps);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    add_counts_kernel<<<1, 32, 0, st>>>(count, (long long*)total);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_jvp: %s", cudaGetErrorString(e));
     return MX_ERR_CUDA;
   }
   return MX_OK;

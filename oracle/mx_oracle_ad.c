@@ -212,6 +212,9 @@ static void d_rates(const mx_network* net, dn Tc, dn nd, const double* Jc, const
       const dn e = dexp(mk(lm[r], dlm ? dlm[r] : 0.0));
       kf[r] = mul(kf[r], e);
       kr[r] = mul(kr[r], e);
+    } else if (dlm) { /* no multipliers: lm = 0, whose tangent still scales both directions */
+      kf[r].d += kf[r].v * dlm[r];
+      kr[r].d += kr[r].v * dlm[r];
     }
   }
 }

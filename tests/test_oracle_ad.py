@@ -165,3 +165,16 @@ def test_non_finite_log_multiplier_fails_the_cell(case):
     for k in ("x", "h", "steps", "flag", "dx"):
         a, b = (r[k][:, 1:] if k == "dx" else r[k][1:]), (good[k][:, 1:] if k == "dx" else good[k][1:])
         assert np.array_equal(a, b), k
+
+
+def test_no_multipliers_are_zero_multipliers(case):
+    # lm None is lm = 0: the tangent along dlm still scales both directions of each reaction
+    o, tab = case["o"], case["tab"]
+    x, T, P, dt, h, J = (case[k] for k in ("x", "T", "P", "dt", "h", "J"))
+    B = x.shape[0]
+    dlm = np.random.default_rng(4).standard_normal((1, B, tab.nr))
+    none = o.jvp(x, T, P, dt, h, dlm=dlm, J=J)
+    zero = o.jvp(x, T, P, dt, h, dlm=dlm, lm=np.zeros((B, tab.nr)), J=J)
+    for k in ("x", "h", "steps", "dx", "dh"):
+        assert np.array_equal(none[k], zero[k]), k
+    assert np.abs(none["dx"]).max() > 0.0
