@@ -184,6 +184,24 @@ int mx_jvp(mx_solver* s, const double* x, const double* T, const double* P, cons
            int32_t* done, double* steps, int32_t* flag, int32_t* status, double* dx_out, double* dh_out,
            int32_t* count, int64_t* total, void* stream, char* err, size_t errlen);
 
+/*
+ * One call and its adjoint (replaces ADSolver.vjp's launches, maxichem/kincuda_ad.py:455-556): the call, guard and
+ * recovery as mx_jvp's, then the cotangents of the inputs for the cotangents gx [B][ns] of x_out and gh [B] of h_out
+ * (NULL for zero; used with adapt 1 only). The forward pass stores each try's state, beyond 2 cap tries a checkpoint
+ * every ceil(n / 2 cap) tries whose segments are recomputed; max_steps may be at most (2 cap)^2 / MX_REC_STEPS.
+ * Outputs as mx_call's, and gx0 [B][ns], gT, gP, gdt, gh0 [B], glm [B][nr], gJ [B][nj] (NULL when nj == 0) per cell,
+ * and grc [nr][9], the rate table's nine Arrhenius columns, summed over the cells in a fixed order. A cell that still
+ * fails (flag 2) has NaN cotangents and is left out of grc, as is a refused cell. Results do not depend on the batch
+ * order or on the launch: no atomics enter the arithmetic. Allocates the adjoint's scratch at the first call and when
+ * a call needs more. Calls run one at a time.
+ */
+int mx_vjp(mx_solver* s, const double* x, const double* T, const double* P, const double* dt, const double* h_in,
+           const double* J, const double* lm, const double* rc, int64_t B, double rtol, double atol, int32_t max_steps,
+           int32_t adapt, int32_t cap, const double* gx, const double* gh, double* x_out, double* h_out, int32_t* done,
+           double* steps, int32_t* flag, int32_t* status, double* gx0, double* gT, double* gP, double* gdt,
+           double* gh0, double* glm, double* grc, double* gJ, int32_t* count, int64_t* total, void* stream,
+           char* err, size_t errlen);
+
 /* The guard alone on given states (replaces a launch of the reference's guard kernel, maxichem/kernels/guard.cuh:114):
  * counts refused cells from status, checks and corrects the others in x_out, writes flag 0/1 and the recompute list
  * count. Device pointers; used by tests of the guard's thresholds. */

@@ -7,7 +7,8 @@ solver module does, on first use.
 
 from .network import VulcanNetwork
 
-__all__ = ["ADSolver", "CudaSolver", "CallResult", "JvpResult", "LaunchResult", "VulcanNetwork"]
+__all__ = ["ADSolver", "CudaSolver", "CallResult", "Cotangents", "JvpResult", "LaunchResult", "VjpResult",
+           "VulcanNetwork"]
 
 
 def __getattr__(name: str):
@@ -15,7 +16,7 @@ def __getattr__(name: str):
         from . import solver
 
         return getattr(solver, name)
-    if name in ("ADSolver", "JvpResult"):
+    if name in ("ADSolver", "Cotangents", "JvpResult", "VjpResult"):
         from . import ad
 
         return getattr(ad, name)

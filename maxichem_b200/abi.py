@@ -117,6 +117,11 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         [_P, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
          ctypes.c_int32, ctypes.c_int32] + [_P] * 8 + [_P] * 10 + [_P, _ERR, ctypes.c_size_t],
     ),  # fmt: skip
+    "mx_vjp": (
+        ctypes.c_int,
+        [_P, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+         ctypes.c_int32, ctypes.c_int32] + [_P] * 18 + [_P, _ERR, ctypes.c_size_t],
+    ),  # fmt: skip
     "mx_guard": (
         ctypes.c_int,
         [_P, _P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_double, _P, _P, _P, _ERR, ctypes.c_size_t],

@@ -18,7 +18,7 @@ from .constants import ARRHENIUS_COLUMNS, ATOL, CAP, DEFAULT_MAX_STEPS, DEFAULT_
 from .network import VulcanNetwork
 from .solver import _ERRLEN, CudaSolver, _ptr, check_inputs, check_photolysis, check_tensor
 
-__all__ = ["ADSolver", "JvpResult"]
+__all__ = ["ADSolver", "Cotangents", "JvpResult", "VjpResult"]
 
 
 class JvpResult(NamedTuple):
@@ -32,6 +32,32 @@ class JvpResult(NamedTuple):
     steps: torch.Tensor
     dx: torch.Tensor
     dh: torch.Tensor
+
+
+class Cotangents(NamedTuple):
+    """The cotangents of ``ADSolver.vjp``'s inputs, float64, each per unit of its input (kincuda_ad.py:63-91): x [B, S];
+    T, P, dt, h [B] (per K, per dyn cm^-2, per s, per s); lm [B, R]; rc [R, 9], the rate table's Arrhenius columns,
+    a sum over the cells; J [B, branches], None without photolysis."""
+
+    x: torch.Tensor
+    T: torch.Tensor
+    P: torch.Tensor
+    dt: torch.Tensor
+    h: torch.Tensor
+    lm: torch.Tensor
+    rc: torch.Tensor
+    J: torch.Tensor | None
+
+
+class VjpResult(NamedTuple):
+    """What ``ADSolver.vjp`` returns (``self.flag`` holds the per-cell flag): x, h, done, steps as
+    ``CudaSolver.launch``, and the ``Cotangents`` of the inputs (kincuda_ad.py:94-108)."""
+
+    x: torch.Tensor
+    h: torch.Tensor
+    done: torch.Tensor
+    steps: torch.Tensor
+    cotangents: Cotangents
 
 
 class ADSolver(CudaSolver):
@@ -139,6 +165,51 @@ class ADSolver(CudaSolver):
         self.flag = flag
         return JvpResult(xo, ho, done.bool(), steps, dxo[0] if one else dxo, dho[0] if one else dho)
 
-    def vjp(self, *args: object, **kwargs: object) -> None:
-        """The adjoint (kincuda_ad.py:455-556) is not built in this library: ``jvp`` gives the tangent."""
-        raise NotImplementedError("ADSolver.vjp: the adjoint is not built in maxichem_b200; use jvp for the tangent")
+    def vjp(self, x: torch.Tensor, T: torch.Tensor, P: torch.Tensor, dt: torch.Tensor, h: torch.Tensor,
+            gx: torch.Tensor, *, gh: torch.Tensor | None = None, lm: torch.Tensor | None = None,
+            rc: torch.Tensor | None = None, adapt: bool = True, rtol: float = DEFAULT_RTOL, atol: float = ATOL,
+            max_steps: int = DEFAULT_MAX_STEPS, J: torch.Tensor | None = None) -> VjpResult:
+        """Run the call and the cotangents of its inputs (kincuda_ad.py:455-556). Everything after gx is keyword only.
+
+        x, T, P, dt, h, lm, rc, adapt, rtol, atol, max_steps and J as ``jvp``; gx [B, S] the cotangent of the output
+        x, gh [B] that of the output h (adaptive only). A cell with flag 2 (``self.flag``) has NaN in its own
+        cotangents and is left out of rc's sum; ``fallback["still_failed"]`` counts the cells left out. Raises
+        ValueError as ``CudaSolver.launch`` if a cell was refused (``self.flag`` is then None).
+        """
+        self.flag = None
+        self._require_open()
+        B = check_inputs(self.dev, self.ns, x, T, P, dt, h, rtol, atol, max_steps)
+        limit = (2 * self.cap) ** 2 // REC_STEPS  # what the recovery's checkpoints reach
+        if max_steps > limit:
+            raise ValueError(f"max_steps: at most {limit} at cap {self.cap} expected, got {max_steps}")
+        if lm is not None:
+            check_tensor("lm", lm, (B, self.nr), self.dev)
+            lm = lm.contiguous()
+        if rc is not None:
+            check_tensor("rc", rc, tuple(self._rc0.shape), self.dev)
+            rc = rc.contiguous()
+        jx = check_photolysis(J, B, self.nj, self.dev)
+        check_tensor("gx", gx, (B, self.ns), self.dev)
+        gx = gx.contiguous()
+        if gh is not None:
+            check_tensor("gh", gh, (B,), self.dev)
+            gh = gh.contiguous()
+        x, T, P, dt, h = (a.contiguous() for a in (x, T, P, dt, h))
+        xo, ho, steps = torch.empty_like(x), torch.empty_like(h), torch.empty_like(h)
+        done, flag, status = (torch.empty(B, dtype=torch.int32, device=self.dev) for _ in range(3))
+        f64 = lambda *shape: torch.empty(*shape, dtype=torch.float64, device=self.dev)  # noqa: E731
+        g = Cotangents(x=torch.empty_like(x), T=f64(B), P=f64(B), dt=f64(B), h=f64(B), lm=f64(B, self.nr),
+                       rc=f64(self.nr, ARRHENIUS_COLUMNS), J=f64(B, self.nj) if self.nj else None)  # fmt: skip
+        stream = torch.cuda.current_stream(self.dev).cuda_stream
+        err = ctypes.create_string_buffer(_ERRLEN)
+        code = self._lib.mx_vjp(
+            self._handle, _ptr(x), _ptr(T), _ptr(P), _ptr(dt), _ptr(h), _ptr(jx), _ptr(lm), _ptr(rc), B, float(rtol),
+            float(atol), int(max_steps), int(bool(adapt)), self.cap, _ptr(gx), _ptr(gh), _ptr(xo), _ptr(ho),
+            _ptr(done), _ptr(steps), _ptr(flag), _ptr(status), _ptr(g.x), _ptr(g.T), _ptr(g.P), _ptr(g.dt),
+            _ptr(g.h), _ptr(g.lm), _ptr(g.rc), _ptr(g.J), _ptr(self.count), _ptr(self.total), stream, err, _ERRLEN,
+        )  # fmt: skip
+        if code:
+            raise (ValueError if code == 1 else RuntimeError)(err.value.decode())
+        self._refuse(x, T, P, dt, jx, status)
+        self.flag = flag
+        return VjpResult(xo, ho, done.bool(), steps, g)

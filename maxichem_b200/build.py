@@ -8,7 +8,7 @@ from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
 SOURCES = [PACKAGE / "csrc" / "maxichem_b200.cu", PACKAGE / "csrc" / "coupling.cu", PACKAGE / "csrc" / "export.cpp"]
-HEADERS = [PACKAGE / "csrc" / "device.cuh", PACKAGE / "csrc" / "jvp.cuh", PACKAGE.parent / "include" / "maxichem_b200.h"]
+HEADERS = [PACKAGE / "csrc" / "device.cuh", PACKAGE / "csrc" / "jvp.cuh", PACKAGE / "csrc" / "vjp.cuh", PACKAGE.parent / "include" / "maxichem_b200.h"]
 OUTPUT = PACKAGE / "_build" / "libmaxichem_b200.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

@@ -582,9 +582,24 @@ struct DeviceScope {
 
 }  // namespace
 
-#include "jvp.cuh"
+#include "vjp.cuh"
 
 namespace {
+
+typedef void (*VjpFn)(const Net, const CallArgs, const AdjArgs, const AdjLayout);
+typedef void (*VjpRecoverFn)(const Net, const CallArgs, const AdjArgs, const AdjLayout, int);
+
+// the adjoint kernels for rows_per_lane R of the warp solves
+bool pick_vjp_kernels(int r, VjpFn* vjp, VjpRecoverFn* rec) {
+  switch (r) {
+    case 1: *vjp = vjp_kernel<WARPS, 1>; *rec = vjp_recover_kernel<WARPS, 1>; return true;
+    case 2: *vjp = vjp_kernel<WARPS, 2>; *rec = vjp_recover_kernel<WARPS, 2>; return true;
+    case 3: *vjp = vjp_kernel<WARPS, 3>; *rec = vjp_recover_kernel<WARPS, 3>; return true;
+    case 4: *vjp = vjp_kernel<WARPS, 4>; *rec = vjp_recover_kernel<WARPS, 4>; return true;
+    case 8: *vjp = vjp_kernel<WARPS, 8>; *rec = vjp_recover_kernel<WARPS, 8>; return true;
+    default: return false;
+  }
+}  // fmt: skip
 
 typedef void (*JvpFn)(const Net, const CallArgs, const TanArgs, const TanLayout);
 typedef void (*JvpRecoverFn)(const Net, const CallArgs, const TanArgs, const TanLayout, int);
@@ -628,6 +643,20 @@ struct mx_solver {
   int jvp_ctas = 0, jvp_recover_ctas = 0;
   double* jvp_scratch = nullptr;
   size_t jvp_scratch_doubles = 0;
+  // the adjoint kernels (set up at the first mx_vjp call)
+  std::vector<uint64_t> rx8_host;  // the reactions' slots, for the species gather table
+  std::vector<uint64_t> st8_host;  // S's columns: per reaction up to 6 (species byte, coefficient code) pairs
+  VjpFn vjp = nullptr;
+  VjpRecoverFn vjp_recover = nullptr;
+  AdjLayout adj_layout{};
+  size_t vjp_smem = 0;
+  int vjp_ctas = 0, vjp_recover_ctas = 0;
+  const int *sp_ptr = nullptr, *sp_ent = nullptr;
+  const uint64_t* st8 = nullptr;
+  double* vjp_scratch = nullptr;
+  size_t vjp_scratch_doubles = 0;
+  double* vjp_gl = nullptr;
+  size_t vjp_gl_doubles = 0;
 };
 
 namespace {
@@ -652,6 +681,12 @@ void release(mx_solver* s) {
   if (s->jvp_scratch) cudaFree(s->jvp_scratch);
   s->jvp_scratch = nullptr;
   s->jvp_scratch_doubles = 0;
+  if (s->vjp_scratch) cudaFree(s->vjp_scratch);
+  s->vjp_scratch = nullptr;
+  s->vjp_scratch_doubles = 0;
+  if (s->vjp_gl) cudaFree(s->vjp_gl);
+  s->vjp_gl = nullptr;
+  s->vjp_gl_doubles = 0;
 }
 
 }  // namespace
@@ -757,6 +792,25 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
     uint64_t w = 0;
     for (int q = 0; q < 6; q++) w |= (uint64_t)n->rx[6 * r + q] << (8 * q);
     rx8[r] = w;
+  }
+  s->rx8_host = rx8;
+  {  // S's columns from its rows' terms: species bytes 0-5 (padding ns), coefficient codes 2 bits each from bit 48
+    std::vector<int> used(nr, 0);
+    s->st8_host.assign(nr, 0);
+    for (int r = 0; r < nr; r++)
+      for (int m = 0; m < 6; m++) s->st8_host[r] |= (uint64_t)ns << (8 * m);
+    for (int i = 0; i < ns; i++)
+      for (int t = n->sv_ptr[i]; t < n->sv_ptr[i + 1]; t++) {
+        const uint32_t w = n->sv_term[t];
+        const int r = (int)(w & 0xffff), m = used[r]++;
+        if (r >= nr || m >= 6) {
+          set_error(err, errlen, "mx_create: reaction %d has more than 6 stoichiometry entries", r);
+          delete s;
+          return MX_ERR_NETWORK;
+        }
+        s->st8_host[r] &= ~((uint64_t)255 << (8 * m));
+        s->st8_host[r] |= (uint64_t)i << (8 * m) | (uint64_t)((w >> 16) & 3) << (48 + 2 * m);
+      }
   }
   const int nsv = n->sv_ptr[ns], njt = n->jac_ptr[n->n_entries];
   if (n->stream_threads[0] != 32 * WARPS || n->stream_threads[1] != 32 * (WARPS - 1)) {
@@ -1235,6 +1289,175 @@ extern "C" int mx_jvp(mx_solver* s, const double* x, const double* T, const doub
   }
   if (e != cudaSuccess) {
     set_error(err, errlen, "mx_jvp: %s", cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  return MX_OK;
+}
+
+// ---- mx_vjp: the call and its adjoint ----
+
+namespace {
+
+// grow a solver-owned device buffer of doubles to at least `need`
+int grow_doubles(double** p, size_t* have, size_t need, const char* what, char* err, size_t errlen) {
+  if (need <= *have) return MX_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  const cudaError_t e = cudaMalloc(p, need * sizeof(double));
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_vjp: the %s of %zu doubles: %s", what, need, cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  *have = need;
+  return MX_OK;
+}
+
+// The adjoint kernels' shared-memory layout, launch limits and species gather table, once per solver.
+int setup_vjp(mx_solver* s, char* err, size_t errlen) {
+  if (s->vjp) return MX_OK;
+  const Net& net = s->net;
+  const int ns = net.ns, nr = net.nr;
+  AdjLayout& l = s->adj_layout;
+  int off = net.doubles;
+  auto take = [&](int doubles) {
+    const int o = off;
+    off += (doubles + 1) & ~1;
+    return o;
+  };
+  l.stride = (ns + 2) & ~1;
+  l.oNb = take(ns + 1);
+  l.oYb = take(ns + 1);
+  l.oFb = take(ns + 1);
+  l.oUb = take(ns + 1);
+  l.oNn = take(ns + 1);
+  l.oNx = take(ns + 1);
+  l.oKb = take(4 * l.stride);
+  l.oBb = take(4 * l.stride);
+  l.oRed = take(32 * WARPS + 2);
+  l.doubles = off;
+  const size_t smem = (size_t)off * sizeof(double);
+  VjpFn vjp = nullptr;
+  VjpRecoverFn rec = nullptr;
+  if (!pick_vjp_kernels(s->rows_per_lane, &vjp, &rec)) {
+    set_error(err, errlen, "mx_vjp: no adjoint kernels for %d rows per lane", s->rows_per_lane);
+    return MX_ERR_NETWORK;
+  }
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
+  if ((size_t)optin < smem) {
+    set_error(err, errlen, "the adjoint kernels need %zu B of shared memory per cell; the device has %d per block",
+              smem, optin);
+    return MX_ERR_NETWORK;
+  }
+  // species j's reaction slots (r * 8 + m), in ascending reaction and slot order
+  std::vector<int> ptr(ns + 1, 0), ent;
+  for (int j = 0; j < ns; j++) {
+    for (int r = 0; r < nr; r++)
+      for (int m = 0; m < 6; m++)
+        if ((int)((s->rx8_host[r] >> (8 * m)) & 255) == j) ent.push_back(r * 8 + m);
+    ptr[j + 1] = (int)ent.size();
+  }
+  cudaError_t e = upload(s, ptr.data(), ptr.size(), &s->sp_ptr);
+  if (e == cudaSuccess) e = upload(s, ent.data(), ent.size(), &s->sp_ent);
+  if (e == cudaSuccess) e = upload(s, s->st8_host.data(), s->st8_host.size(), &s->st8);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)vjp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)rec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int a = 0, b = 0;
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (const void*)vjp, 32 * WARPS, smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)rec, 32 * WARPS, smem);
+  if (e == cudaSuccess && (a < 1 || b < 1)) e = cudaErrorInvalidConfiguration;
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_vjp: %s", cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  s->vjp_smem = smem;
+  s->vjp_ctas = a;
+  s->vjp_recover_ctas = b;
+  s->vjp = vjp;
+  s->vjp_recover = rec;
+  return MX_OK;
+}
+
+}  // namespace
+
+extern "C" int mx_vjp(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
+                      const double* h_in, const double* J, const double* lm, const double* rc, int64_t B, double rtol,
+                      double atol, int32_t max_steps, int32_t adapt, int32_t cap, const double* gx, const double* gh,
+                      double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag, int32_t* status,
+                      double* gx0, double* gT, double* gP, double* gdt, double* gh0, double* glm, double* grc,
+                      double* gJ, int32_t* count, int64_t* total, void* stream, char* err, size_t errlen) {
+  if (!s) {
+    set_error(err, errlen, "this solver was closed; build a new one");
+    return MX_ERR_CLOSED;
+  }
+  if (B < 0 || B > 0x7fffffff) {
+    set_error(err, errlen, "mx_vjp: B out of range: %lld", (long long)B);
+    return MX_ERR_ARGUMENT;
+  }
+  if (!(rtol > 0.0 && rtol < 1e300 && atol > 0.0 && atol < 1e300)) {
+    set_error(err, errlen, "rtol and atol finite and positive expected, got %g, %g", rtol, atol);
+    return MX_ERR_ARGUMENT;
+  }
+  if (cap < 1 || cap > 100000 || (adapt != 0 && adapt != 1)) {
+    set_error(err, errlen, "mx_vjp: cap from 1 to 100000 and adapt 0 or 1 expected, got %d and %d", cap, adapt);
+    return MX_ERR_ARGUMENT;
+  }
+  const int64_t reach = (int64_t)(2 * cap) * (2 * cap) / MX_REC_STEPS;  // what the recovery's checkpoints reach
+  if (max_steps < 1 || max_steps > reach) {
+    set_error(err, errlen, "max_steps: at most %lld at cap %d expected, got %d", (long long)reach, cap, max_steps);
+    return MX_ERR_ARGUMENT;
+  }
+  if (!count || !total || (B > 0 && (!x || !T || !P || !dt || !h_in || !x_out || !h_out || !done || !steps ||
+                                     !flag || !status || (s->net.nj > 0 && (!J || !gJ)) || !gx || !gx0 || !gT ||
+                                     !gP || !gdt || !gh0 || !glm || !grc))) {
+    set_error(err, errlen, "mx_vjp: a required array is null");
+    return MX_ERR_ARGUMENT;
+  }
+  DeviceScope scope(s->device);
+  if (scope.status != cudaSuccess) {
+    set_error(err, errlen, "mx_vjp: device %d: %s", s->device, cudaGetErrorString(scope.status));
+    return MX_ERR_CUDA;
+  }
+  int rcode = setup_vjp(s, err, errlen);
+  if (rcode) return rcode;
+  rcode = grow_list(s, std::max<int64_t>(B, 1), err, errlen);
+  if (rcode) return rcode;
+  const Net& n0 = s->net;
+  const int stored = 2 * cap;
+  const long long slot = ((long long)14 * n0.nr + 2LL * stored * (n0.ns + REC_EXTRA) + 1) & ~1ll;
+  const int grid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)s->vjp_ctas * s->sms);
+  const int rgrid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)s->vjp_recover_ctas * s->sms);
+  rcode = grow_doubles(&s->vjp_scratch, &s->vjp_scratch_doubles, (size_t)std::max(grid, rgrid) * (size_t)slot,
+                       "adjoint scratch", err, errlen);
+  if (rcode) return rcode;
+  rcode = grow_doubles(&s->vjp_gl, &s->vjp_gl_doubles, (size_t)std::max<int64_t>(B, 1) * n0.nr * 3,
+                       "per-cell rate-table cotangents", err, errlen);
+  if (rcode) return rcode;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
+  if (e == cudaSuccess && B > 0) {
+    Net net = s->net;
+    if (rc) net.rc = rc;  // the caller's rate table
+    const CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status,
+                     count, s->list, nullptr};
+    const AdjArgs aa{lm, gx, gh, adapt, stored, gx0, gT, gP, gdt, gh0, glm, s->net.nj > 0 ? gJ : nullptr,
+                     s->vjp_gl, s->vjp_scratch, slot, s->sp_ptr, s->sp_ent, s->st8};
+    s->vjp<<<grid, 32 * WARPS, s->vjp_smem, st>>>(net, a, aa, s->adj_layout);
+    s->vjp_recover<<<rgrid, 32 * WARPS, s->vjp_smem, st>>>(net, a, aa, s->adj_layout, MX_REC_STEPS * max_steps);
+    arrh_kernel<<<n0.nr, ARRH_THREADS, 0, st>>>(net, a, s->vjp_gl, grc);
+    e = cudaGetLastError();
+  } else if (e == cudaSuccess) {
+    e = cudaMemsetAsync(grc, 0, (size_t)n0.nr * 9 * sizeof(double), st);
+  }
+  if (e == cudaSuccess) {
+    add_counts_kernel<<<1, 32, 0, st>>>(count, (long long*)total);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_vjp: %s", cudaGetErrorString(e));
     return MX_ERR_CUDA;
   }
   return MX_OK;
