@@ -7,6 +7,7 @@ step is then the fifth 300 s call (x, T, P, dt, h, J resident in HBM), repeated 
 (552 MB of x alone) exceed L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--cells B] [--impl ours|reference]
+  python bench.py --derivative jvp|vjp [--directions D] [--frozen] [--cells B]   (the derivative calls)
 
 --impl reference times the CPU implementation of the same solve (the oracle, a C restatement of the reference's
 kernels, on all host threads) on a bounded sample of the same cells; rank 0 alone runs it.
@@ -55,6 +56,10 @@ def parse() -> argparse.Namespace:
     p.add_argument("--network", choices=("cho41", "chno69", "sncho91"), default=NETWORK,
                    help="the synthetic network (the metric is quoted on chno69)")
     p.add_argument("--dt", type=float, default=DT, help="the call's dt, s (300; the sulfur configuration uses 600)")
+    p.add_argument("--derivative", choices=("jvp", "vjp"), default=None,
+                   help="time the call with its tangent (jvp, --directions of them) or its adjoint (vjp) instead")
+    p.add_argument("--directions", type=int, default=1, help="tangent directions of --derivative jvp")
+    p.add_argument("--frozen", action="store_true", help="--derivative with adapt=False (the accepted steps held)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -153,6 +158,9 @@ def main() -> None:
         return
     if args.workload == "uneven":
         run_uneven(args)
+        return
+    if args.derivative:
+        run_derivative(args)
         return
     import torch
     import torch.distributed as dist
@@ -255,6 +263,76 @@ def main() -> None:
     solver.close()
     if world > 1:
         dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_derivative(args) -> None:
+    """cells/s of the call with its tangent (ADSolver.jvp along --directions seeded directions of every input class)
+    or its adjoint (ADSolver.vjp of seeded cotangents of x and h), on the settled column workload of the default line;
+    the plain call is timed beside it on the same inputs."""
+    import torch
+
+    from maxichem_b200 import replicas, synthetic
+    from maxichem_b200.ad import ADSolver
+
+    rank, local, world = replicas.rank_from_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    net = synthetic.network(args.network)
+    B = args.cells
+    w = inputs(net, B, seed=replicas.seed(1000, rank))
+    w.dt[:] = args.dt
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    solver = ADSolver(net, dev, photo=True)
+    x, T, P, dt, h, J = t(w.x), t(w.T), t(w.P), t(w.dt), t(w.h), t(w.J)
+    for _ in range(SPINUP_CALLS):
+        x, h, _, _ = solver(x, T, P, dt, h, J=J)
+    rng = np.random.default_rng(7)
+    ns, nr, nj, D = solver.ns, solver.nr, solver.nj, args.directions
+    adapt = not args.frozen
+    if args.derivative == "jvp":
+        xs = x.cpu().numpy()
+        dx = xs * rng.standard_normal((D, B, ns))
+        dx -= xs * dx.sum(2, keepdims=True)
+        tan = [t(dx)] + [t(rng.standard_normal((D, B)) * s) for s in (w.T * 0.01, w.P, w.dt, h.cpu().numpy())]
+        extra = dict(dlm=t(rng.standard_normal((D, B, nr))), dJ=t(w.J * rng.standard_normal((D, B, nj))))
+        run = lambda: solver.jvp(x, T, P, dt, h, *tan, J=J, adapt=adapt, **extra)  # noqa: E731
+    else:
+        gx = t(rng.standard_normal((B, ns)) / np.maximum(x.cpu().numpy(), 1e-20))
+        gh = t(rng.standard_normal(B)) if adapt else None
+        run = lambda: solver.vjp(x, T, P, dt, h, gx, gh=gh, J=J, adapt=adapt)  # noqa: E731
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn) -> float:
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / args.steps
+
+    with Clocks(local) as clocks:
+        ms = timed(run)
+    flags = np.bincount(solver.flag.cpu().numpy(), minlength=3).tolist()
+    ms_call = timed(lambda: solver.launch(x, T, P, dt, h, J=J))
+    what = f"its tangent along {D} direction{'s' if D > 1 else ''}" if args.derivative == "jvp" else "its adjoint"
+    line = {
+        "metric": f"cells/s per GCM call with {what} ({solver.ns}-sp, {B * world} cells, dt {args.dt:g} s): FP64",
+        "value": replicas.throughput(B, world, ms * 1e-3), "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded network and column grid)",
+        "config": {"workload": f"{args.network}: call {SPINUP_CALLS + 1} of {args.dt:g} s calls on a {LEVELS}-level "
+                               "column grid", "derivative": args.derivative,
+                   "directions": D if args.derivative == "jvp" else None,
+                   "contract": "adaptive" if adapt else "frozen", "cells_per_gpu": B, "flags": flags},
+        "call_ms_per_step": ms_call, "cost_vs_call": ms / ms_call, "clocks": clocks.summary(),
+    }  # fmt: skip
+    solver.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
