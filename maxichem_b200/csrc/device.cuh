@@ -611,7 +611,7 @@ __device__ __forceinline__ double step_factor(double en, bool ok, bool prej, dou
 }
 
 // err of a try on warp 0 (try_error, common.cuh:570-590): Y = N + 2 K1 + K3 + K4; writes en and ok to red[0..1].
-__device__ void try_error(const Net& net, const Cell& c, bool first, double rtol, double atol, int lane) {
+static __device__ void try_error(const Net& net, const Cell& c, bool first, double rtol, double atol, int lane) {
   double e2 = 0.0, em = 0.0;
   bool nn = true;
   for (int i = lane; i < net.ns; i += 32) {
@@ -648,7 +648,7 @@ __host__ __device__ constexpr int guard_scratch(int ns) {
 // renormalised. Every sum runs over the species in network order, one lane per sum, as the reference's one thread
 // per cell adds them, so each sum has the reference's bits. at: atoms [ns][nel]; scr: guard_scratch(ns) doubles of
 // shared memory, free during the guard.
-__device__ __noinline__ int check_cell(const Net& net, const double* x0, double* xo, int done, double nok,
+static __device__ __noinline__ int check_cell(const Net& net, const double* x0, double* xo, int done, double nok,
                                        double atol, int lane, const double* at, double* scr) {
   constexpr int ME = MX_MAX_ELEMENTS;
   const int ns = net.ns, nel = net.nel;
@@ -739,6 +739,18 @@ __device__ __noinline__ int check_cell(const Net& net, const double* x0, double*
   for (int i = lane; i < ns; i += 32) xo[i] *= is;
   __syncwarp();
   return 0;
+}
+
+// The guard's inputs into the matrix's space, free once the steps are done: atoms [ns][nel] and the cell's input row,
+// so the guard's species sums read shared memory. Falls back to global memory when they do not fit.
+__device__ __forceinline__ void stage_guard_inputs(const Net& net, const Cell& c, const double* x0, int tid, int nt,
+                                                   const double** at, const double** xin) {
+  const int ns = net.ns, na = ns * net.nel;
+  if (na + ns > ns * net.ld) return;
+  for (int e = tid; e < na; e += nt) c.A[e] = __ldg(net.atoms + e);
+  for (int i = tid; i < ns; i += nt) c.A[na + i] = x0[i];
+  *at = c.A;
+  *xin = c.A + na;
 }
 
 }  // namespace mx

@@ -15,25 +15,11 @@
 #include <new>
 #include <vector>
 
-#include "device.cuh"
+#include "solver.cuh"
 
 using namespace mx;
 
 namespace {
-
-constexpr int WARPS = 4;  // warps per cell
-
-// The guard's inputs into the matrix's space, free once the steps are done: atoms [ns][nel] and the cell's input row,
-// so the guard's species sums read shared memory. Falls back to global memory when they do not fit.
-__device__ __forceinline__ void stage_guard_inputs(const Net& net, const Cell& c, const double* x0, int tid, int nt,
-                                                   const double** at, const double** xin) {
-  const int ns = net.ns, na = ns * net.nel;
-  if (na + ns > ns * net.ld) return;
-  for (int e = tid; e < na; e += nt) c.A[e] = __ldg(net.atoms + e);
-  for (int i = tid; i < ns; i += nt) c.A[na + i] = x0[i];
-  *at = c.A;
-  *xin = c.A + na;
-}
 
 // Phases of a try that the profiling variant of the call kernel times (clock64 on thread 0, summed over cells).
 enum { PH_RATES, PH_RHS_JAC, PH_LU, PH_STAGE12, PH_STAGE3, PH_STAGE4, PH_CONTROL, PH_OUTPUT, PH_COUNT };
@@ -527,17 +513,6 @@ __global__ void __launch_bounds__(128) guard_kernel(const Net net, const double*
   flag[cell] = r;
 }
 
-__global__ void add_counts_kernel(const int* count, long long* total) {
-  const int i = (int)threadIdx.x;
-  if (i < MX_COUNT_SLOTS) total[i] += count[i];
-}
-
-typedef void (*CallFn)(const Net, const CallArgs, long long*);
-typedef void (*DebugFn)(const Net, const double*, double, double, double, const double*, double, double, double*);
-typedef void (*RecoverFn)(const Net, const CallArgs, int);
-typedef void (*TimeFn)(const Net, const double*, double, double, double, const double*, int, long long*);
-
-
 template <int R>
 void kernels_for(CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg, TimeFn* tim) {
   *tim = time_phases_kernel<WARPS, R>;
@@ -558,135 +533,16 @@ bool pick_kernels(int ns, CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* d
   return false;
 }
 
-void set_error(char* err, size_t len, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
-void set_error(char* err, size_t len, const char* fmt, ...) {
-  if (!err || !len) return;
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(err, len, fmt, ap);
-  va_end(ap);
-}
-
-// Restores the caller's current device on scope exit.
-struct DeviceScope {
-  int old = -1;
-  cudaError_t status;
-  explicit DeviceScope(int dev) {
-    cudaGetDevice(&old);
-    status = cudaSetDevice(dev);
-  }
-  ~DeviceScope() {
-    if (old >= 0) cudaSetDevice(old);
-  }
-};
-
 }  // namespace
 
-#include "vjp.cuh"
-
 namespace {
-
-typedef void (*VjpFn)(const Net, const CallArgs, const AdjArgs, const AdjLayout);
-typedef void (*VjpRecoverFn)(const Net, const CallArgs, const AdjArgs, const AdjLayout, int);
-
-// the adjoint kernels for rows_per_lane R of the warp solves
-bool pick_vjp_kernels(int r, VjpFn* vjp, VjpRecoverFn* rec) {
-  switch (r) {
-    case 1: *vjp = vjp_kernel<WARPS, 1>; *rec = vjp_recover_kernel<WARPS, 1>; return true;
-    case 2: *vjp = vjp_kernel<WARPS, 2>; *rec = vjp_recover_kernel<WARPS, 2>; return true;
-    case 3: *vjp = vjp_kernel<WARPS, 3>; *rec = vjp_recover_kernel<WARPS, 3>; return true;
-    case 4: *vjp = vjp_kernel<WARPS, 4>; *rec = vjp_recover_kernel<WARPS, 4>; return true;
-    case 8: *vjp = vjp_kernel<WARPS, 8>; *rec = vjp_recover_kernel<WARPS, 8>; return true;
-    default: return false;
-  }
-}  // fmt: skip
-
-typedef void (*JvpFn)(const Net, const CallArgs, const TanArgs, const TanLayout);
-typedef void (*JvpRecoverFn)(const Net, const CallArgs, const TanArgs, const TanLayout, int);
-
-// the tangent kernels for rows_per_lane R of the warp solves
-bool pick_jvp_kernels(int r, JvpFn* jvp, JvpRecoverFn* rec) {
-  switch (r) {
-    case 1: *jvp = jvp_kernel<WARPS, 1>; *rec = jvp_recover_kernel<WARPS, 1>; return true;
-    case 2: *jvp = jvp_kernel<WARPS, 2>; *rec = jvp_recover_kernel<WARPS, 2>; return true;
-    case 3: *jvp = jvp_kernel<WARPS, 3>; *rec = jvp_recover_kernel<WARPS, 3>; return true;
-    case 4: *jvp = jvp_kernel<WARPS, 4>; *rec = jvp_recover_kernel<WARPS, 4>; return true;
-    case 8: *jvp = jvp_kernel<WARPS, 8>; *rec = jvp_recover_kernel<WARPS, 8>; return true;
-    default: return false;
-  }
-}  // fmt: skip
-
-}  // namespace
-
-struct mx_solver {
-  int device = 0;
-  Net net{};
-  std::vector<void*> buffers;
-  CallFn call = nullptr;
-  CallFn call_prof = nullptr;
-  RecoverFn recover = nullptr;
-  DebugFn debug = nullptr;
-  TimeFn timer = nullptr;
-  int rows_per_lane = 0;
-  size_t smem = 0;
-  int sms = 0, call_ctas = 0, recover_ctas = 0;
-  int grid_ctas = -1;  // call-kernel CTAs per SM: 1..call_ctas persistent, 0 one CTA per cell; -1 call_ctas
-  int* list = nullptr;
-  int64_t list_capacity = 0;
-  unsigned long long* tries = nullptr;
-  long long* phases = nullptr;
-  // the tangent kernels (set up at the first mx_jvp call)
-  JvpFn jvp = nullptr;
-  JvpRecoverFn jvp_recover = nullptr;
-  TanLayout tan_layout{};
-  size_t jvp_smem = 0;
-  int jvp_ctas = 0, jvp_recover_ctas = 0;
-  double* jvp_scratch = nullptr;
-  size_t jvp_scratch_doubles = 0;
-  // the adjoint kernels (set up at the first mx_vjp call)
-  std::vector<uint64_t> rx8_host;  // the reactions' slots, for the species gather table
-  std::vector<uint64_t> st8_host;  // S's columns: per reaction up to 6 (species byte, coefficient code) pairs
-  VjpFn vjp = nullptr;
-  VjpRecoverFn vjp_recover = nullptr;
-  AdjLayout adj_layout{};
-  size_t vjp_smem = 0;
-  int vjp_ctas = 0, vjp_recover_ctas = 0;
-  const int *sp_ptr = nullptr, *sp_ent = nullptr;
-  const uint64_t* st8 = nullptr;
-  double* vjp_scratch = nullptr;
-  size_t vjp_scratch_doubles = 0;
-  double* vjp_gl = nullptr;
-  size_t vjp_gl_doubles = 0;
-};
-
-namespace {
-
-template <typename T>
-cudaError_t upload(mx_solver* s, const T* host, size_t count, const T** dev) {
-  void* p = nullptr;
-  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-  cudaError_t e = cudaMalloc(&p, bytes);
-  if (e != cudaSuccess) return e;
-  s->buffers.push_back(p);
-  if (count) e = cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice);
-  *dev = (const T*)p;
-  return e;
-}
 
 void release(mx_solver* s) {
   for (void* p : s->buffers) cudaFree(p);
   s->buffers.clear();
   if (s->list) cudaFree(s->list);
   s->list = nullptr;
-  if (s->jvp_scratch) cudaFree(s->jvp_scratch);
-  s->jvp_scratch = nullptr;
-  s->jvp_scratch_doubles = 0;
-  if (s->vjp_scratch) cudaFree(s->vjp_scratch);
-  s->vjp_scratch = nullptr;
-  s->vjp_scratch_doubles = 0;
-  if (s->vjp_gl) cudaFree(s->vjp_gl);
-  s->vjp_gl = nullptr;
-  s->vjp_gl_doubles = 0;
+  mx_release_derivatives(s);
 }
 
 }  // namespace
@@ -860,20 +716,6 @@ static int call_grid(const mx_solver* s, int64_t B) {
   if (s->grid_ctas == 0) return (int)B;
   const int per_sm = s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas;
   return (int)std::min<int64_t>(B, (int64_t)per_sm * s->sms);
-}
-
-static int grow_list(mx_solver* s, int64_t B, char* err, size_t errlen) {
-  if (B <= s->list_capacity) return MX_OK;
-  if (s->list) cudaFree(s->list);
-  s->list = nullptr;
-  s->list_capacity = 0;
-  const cudaError_t e = cudaMalloc(&s->list, (size_t)B * sizeof(int));
-  if (e != cudaSuccess) {
-    set_error(err, errlen, "mx_call: the recompute list of %lld cells: %s", (long long)B, cudaGetErrorString(e));
-    return MX_ERR_CUDA;
-  }
-  s->list_capacity = B;
-  return MX_OK;
 }
 
 extern "C" int mx_call(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
@@ -1145,319 +987,6 @@ extern "C" int mx_call_static(mx_solver* s, const double* x, const double* T, co
   }
   if (e != cudaSuccess) {
     set_error(err, errlen, "mx_call_static: %s", cudaGetErrorString(e));
-    return MX_ERR_CUDA;
-  }
-  return MX_OK;
-}
-
-// ---- mx_jvp: the call and its tangent ----
-
-namespace {
-
-// The tangent kernels' shared-memory layout and launch limits, once per solver.
-int setup_jvp(mx_solver* s, char* err, size_t errlen) {
-  if (s->jvp) return MX_OK;
-  const Net& net = s->net;
-  const int ns = net.ns, nr = net.nr;
-  TanLayout& l = s->tan_layout;
-  int off = net.doubles;
-  auto take = [&](int doubles) {
-    const int o = off;
-    off += (doubles + 1) & ~1;
-    return o;
-  };
-  l.stride = (ns + 2) & ~1;
-  l.oTN = take(ns + 1);
-  l.oTn = take(ns + 1);
-  l.oTF = take(ns + 1);
-  l.oTu = take(ns + 1);
-  l.oTY = take(ns + 1);
-  l.oJK = take(4 * l.stride);
-  l.oTK = take(4 * l.stride);
-  l.oZ = take(std::max(nr, ns) + 1);
-  l.doubles = off;
-  const size_t smem = (size_t)off * sizeof(double);
-  JvpFn jvp = nullptr;
-  JvpRecoverFn rec = nullptr;
-  if (!pick_jvp_kernels(s->rows_per_lane, &jvp, &rec)) {
-    set_error(err, errlen, "mx_jvp: no tangent kernels for %d rows per lane", s->rows_per_lane);
-    return MX_ERR_NETWORK;
-  }
-  int optin = 0;
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
-  if ((size_t)optin < smem) {
-    set_error(err, errlen, "the tangent kernels need %zu B of shared memory per cell; the device has %d per block",
-              smem, optin);
-    return MX_ERR_NETWORK;
-  }
-  cudaError_t e = cudaFuncSetAttribute((const void*)jvp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)rec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int a = 0, b = 0;
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (const void*)jvp, 32 * WARPS, smem);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)rec, 32 * WARPS, smem);
-  if (e == cudaSuccess && (a < 1 || b < 1)) e = cudaErrorInvalidConfiguration;
-  if (e != cudaSuccess) {
-    set_error(err, errlen, "mx_jvp: %s", cudaGetErrorString(e));
-    return MX_ERR_CUDA;
-  }
-  s->jvp_smem = smem;
-  s->jvp_ctas = a;
-  s->jvp_recover_ctas = b;
-  s->jvp = jvp;
-  s->jvp_recover = rec;
-  return MX_OK;
-}
-
-}  // namespace
-
-extern "C" int mx_jvp(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
-                      const double* h_in, const double* J, const double* lm, const double* rc, int64_t B, double rtol,
-                      double atol, int32_t max_steps, int32_t adapt, int32_t D, const double* dx, const double* dT,
-                      const double* dP, const double* ddt, const double* dh, const double* dlm, const double* drc,
-                      const double* dJ, double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag,
-                      int32_t* status, double* dx_out, double* dh_out, int32_t* count, int64_t* total, void* stream,
-                      char* err, size_t errlen) {
-  if (!s) {
-    set_error(err, errlen, "this solver was closed; build a new one");
-    return MX_ERR_CLOSED;
-  }
-  if (B < 0 || B > 0x7fffffff) {
-    set_error(err, errlen, "mx_jvp: B out of range: %lld", (long long)B);
-    return MX_ERR_ARGUMENT;
-  }
-  if (!(rtol > 0.0 && rtol < 1e300 && atol > 0.0 && atol < 1e300)) {
-    set_error(err, errlen, "rtol and atol finite and positive expected, got %g, %g", rtol, atol);
-    return MX_ERR_ARGUMENT;
-  }
-  if (max_steps < 1 || (int64_t)MX_REC_STEPS * max_steps > 0x7fffffff) {
-    set_error(err, errlen, "max_steps from 1 to %d expected, got %d", 0x7fffffff / MX_REC_STEPS, max_steps);
-    return MX_ERR_ARGUMENT;
-  }
-  if (D < 1 || D > MX_JVP_MAX_DIRECTIONS || (adapt != 0 && adapt != 1)) {
-    set_error(err, errlen, "mx_jvp: from 1 to %d directions and adapt 0 or 1 expected, got %d and %d",
-              MX_JVP_MAX_DIRECTIONS, D, adapt);
-    return MX_ERR_ARGUMENT;
-  }
-  if (!count || !total || (B > 0 && (!x || !T || !P || !dt || !h_in || !x_out || !h_out || !done || !steps ||
-                                     !flag || !status || (s->net.nj > 0 && !J) || !dx || !dT || !dP || !ddt ||
-                                     !dh || !dx_out || !dh_out))) {
-    set_error(err, errlen, "mx_jvp: a required array is null");
-    return MX_ERR_ARGUMENT;
-  }
-  DeviceScope scope(s->device);
-  if (scope.status != cudaSuccess) {
-    set_error(err, errlen, "mx_jvp: device %d: %s", s->device, cudaGetErrorString(scope.status));
-    return MX_ERR_CUDA;
-  }
-  int rcode = setup_jvp(s, err, errlen);
-  if (rcode) return rcode;
-  rcode = grow_list(s, std::max<int64_t>(B, 1), err, errlen);
-  if (rcode) return rcode;
-  const Net& n0 = s->net;
-  const long long slot = ((long long)D * (2 * n0.nr + 2 + n0.ns + 1 + 4) + 1) & ~1ll;
-  const int grid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)s->jvp_ctas * s->sms);
-  const int rgrid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)s->jvp_recover_ctas * s->sms);
-  const size_t need = (size_t)std::max(grid, rgrid) * (size_t)slot;
-  if (need > s->jvp_scratch_doubles) {
-    if (s->jvp_scratch) cudaFree(s->jvp_scratch);
-    s->jvp_scratch = nullptr;
-    s->jvp_scratch_doubles = 0;
-    const cudaError_t e = cudaMalloc(&s->jvp_scratch, need * sizeof(double));
-    if (e != cudaSuccess) {
-      set_error(err, errlen, "mx_jvp: the tangent scratch of %zu doubles: %s", need, cudaGetErrorString(e));
-      return MX_ERR_CUDA;
-    }
-    s->jvp_scratch_doubles = need;
-  }
-  cudaStream_t st = (cudaStream_t)stream;
-  cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
-  if (e == cudaSuccess && B > 0) {
-    Net net = s->net;
-    if (rc) net.rc = rc;  // the caller's rate table
-    const CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status,
-                     count, s->list, nullptr};
-    const TanArgs ta{lm, dx, dT, dP, ddt, dh, dlm, drc, s->net.nj > 0 ? dJ : nullptr, D, adapt, dx_out, dh_out,
-                     s->jvp_scratch, slot};
-    s->jvp<<<grid, 32 * WARPS, s->jvp_smem, st>>>(net, a, ta, s->tan_layout);
-    s->jvp_recover<<<rgrid, 32 * WARPS, s->jvp_smem, st>>>(net, a, ta, s->tan_layout, MX_REC_STEPS * max_steps);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess) {
-    add_counts_kernel<<<1, 32, 0, st>>>(count, (long long*)total);
-    e = cudaGetLastError();
-  }
-  if (e != cudaSuccess) {
-    set_error(err, errlen, "mx_jvp: %s", cudaGetErrorString(e));
-    return MX_ERR_CUDA;
-  }
-  return MX_OK;
-}
-
-// ---- mx_vjp: the call and its adjoint ----
-
-namespace {
-
-// grow a solver-owned device buffer of doubles to at least `need`
-int grow_doubles(double** p, size_t* have, size_t need, const char* what, char* err, size_t errlen) {
-  if (need <= *have) return MX_OK;
-  if (*p) cudaFree(*p);
-  *p = nullptr;
-  *have = 0;
-  const cudaError_t e = cudaMalloc(p, need * sizeof(double));
-  if (e != cudaSuccess) {
-    set_error(err, errlen, "mx_vjp: the %s of %zu doubles: %s", what, need, cudaGetErrorString(e));
-    return MX_ERR_CUDA;
-  }
-  *have = need;
-  return MX_OK;
-}
-
-// The adjoint kernels' shared-memory layout, launch limits and species gather table, once per solver.
-int setup_vjp(mx_solver* s, char* err, size_t errlen) {
-  if (s->vjp) return MX_OK;
-  const Net& net = s->net;
-  const int ns = net.ns, nr = net.nr;
-  AdjLayout& l = s->adj_layout;
-  int off = net.doubles;
-  auto take = [&](int doubles) {
-    const int o = off;
-    off += (doubles + 1) & ~1;
-    return o;
-  };
-  l.stride = (ns + 2) & ~1;
-  l.oNb = take(ns + 1);
-  l.oYb = take(ns + 1);
-  l.oFb = take(ns + 1);
-  l.oUb = take(ns + 1);
-  l.oNn = take(ns + 1);
-  l.oNx = take(ns + 1);
-  l.oKb = take(4 * l.stride);
-  l.oBb = take(4 * l.stride);
-  l.oRed = take(32 * WARPS + 2);
-  l.doubles = off;
-  const size_t smem = (size_t)off * sizeof(double);
-  VjpFn vjp = nullptr;
-  VjpRecoverFn rec = nullptr;
-  if (!pick_vjp_kernels(s->rows_per_lane, &vjp, &rec)) {
-    set_error(err, errlen, "mx_vjp: no adjoint kernels for %d rows per lane", s->rows_per_lane);
-    return MX_ERR_NETWORK;
-  }
-  int optin = 0;
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
-  if ((size_t)optin < smem) {
-    set_error(err, errlen, "the adjoint kernels need %zu B of shared memory per cell; the device has %d per block",
-              smem, optin);
-    return MX_ERR_NETWORK;
-  }
-  // species j's reaction slots (r * 8 + m), in ascending reaction and slot order
-  std::vector<int> ptr(ns + 1, 0), ent;
-  for (int j = 0; j < ns; j++) {
-    for (int r = 0; r < nr; r++)
-      for (int m = 0; m < 6; m++)
-        if ((int)((s->rx8_host[r] >> (8 * m)) & 255) == j) ent.push_back(r * 8 + m);
-    ptr[j + 1] = (int)ent.size();
-  }
-  cudaError_t e = upload(s, ptr.data(), ptr.size(), &s->sp_ptr);
-  if (e == cudaSuccess) e = upload(s, ent.data(), ent.size(), &s->sp_ent);
-  if (e == cudaSuccess) e = upload(s, s->st8_host.data(), s->st8_host.size(), &s->st8);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)vjp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)rec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int a = 0, b = 0;
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (const void*)vjp, 32 * WARPS, smem);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)rec, 32 * WARPS, smem);
-  if (e == cudaSuccess && (a < 1 || b < 1)) e = cudaErrorInvalidConfiguration;
-  if (e != cudaSuccess) {
-    set_error(err, errlen, "mx_vjp: %s", cudaGetErrorString(e));
-    return MX_ERR_CUDA;
-  }
-  s->vjp_smem = smem;
-  s->vjp_ctas = a;
-  s->vjp_recover_ctas = b;
-  s->vjp = vjp;
-  s->vjp_recover = rec;
-  return MX_OK;
-}
-
-}  // namespace
-
-extern "C" int mx_vjp(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
-                      const double* h_in, const double* J, const double* lm, const double* rc, int64_t B, double rtol,
-                      double atol, int32_t max_steps, int32_t adapt, int32_t cap, const double* gx, const double* gh,
-                      double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag, int32_t* status,
-                      double* gx0, double* gT, double* gP, double* gdt, double* gh0, double* glm, double* grc,
-                      double* gJ, int32_t* count, int64_t* total, void* stream, char* err, size_t errlen) {
-  if (!s) {
-    set_error(err, errlen, "this solver was closed; build a new one");
-    return MX_ERR_CLOSED;
-  }
-  if (B < 0 || B > 0x7fffffff) {
-    set_error(err, errlen, "mx_vjp: B out of range: %lld", (long long)B);
-    return MX_ERR_ARGUMENT;
-  }
-  if (!(rtol > 0.0 && rtol < 1e300 && atol > 0.0 && atol < 1e300)) {
-    set_error(err, errlen, "rtol and atol finite and positive expected, got %g, %g", rtol, atol);
-    return MX_ERR_ARGUMENT;
-  }
-  if (cap < 1 || cap > 100000 || (adapt != 0 && adapt != 1)) {
-    set_error(err, errlen, "mx_vjp: cap from 1 to 100000 and adapt 0 or 1 expected, got %d and %d", cap, adapt);
-    return MX_ERR_ARGUMENT;
-  }
-  const int64_t reach = (int64_t)(2 * cap) * (2 * cap) / MX_REC_STEPS;  // what the recovery's checkpoints reach
-  if (max_steps < 1 || max_steps > reach) {
-    set_error(err, errlen, "max_steps: at most %lld at cap %d expected, got %d", (long long)reach, cap, max_steps);
-    return MX_ERR_ARGUMENT;
-  }
-  if (!count || !total || (B > 0 && (!x || !T || !P || !dt || !h_in || !x_out || !h_out || !done || !steps ||
-                                     !flag || !status || (s->net.nj > 0 && (!J || !gJ)) || !gx || !gx0 || !gT ||
-                                     !gP || !gdt || !gh0 || !glm || !grc))) {
-    set_error(err, errlen, "mx_vjp: a required array is null");
-    return MX_ERR_ARGUMENT;
-  }
-  DeviceScope scope(s->device);
-  if (scope.status != cudaSuccess) {
-    set_error(err, errlen, "mx_vjp: device %d: %s", s->device, cudaGetErrorString(scope.status));
-    return MX_ERR_CUDA;
-  }
-  int rcode = setup_vjp(s, err, errlen);
-  if (rcode) return rcode;
-  rcode = grow_list(s, std::max<int64_t>(B, 1), err, errlen);
-  if (rcode) return rcode;
-  const Net& n0 = s->net;
-  const int stored = 2 * cap;
-  const long long slot = ((long long)14 * n0.nr + 2LL * stored * (n0.ns + REC_EXTRA) + 1) & ~1ll;
-  const int grid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)s->vjp_ctas * s->sms);
-  const int rgrid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)s->vjp_recover_ctas * s->sms);
-  rcode = grow_doubles(&s->vjp_scratch, &s->vjp_scratch_doubles, (size_t)std::max(grid, rgrid) * (size_t)slot,
-                       "adjoint scratch", err, errlen);
-  if (rcode) return rcode;
-  rcode = grow_doubles(&s->vjp_gl, &s->vjp_gl_doubles, (size_t)std::max<int64_t>(B, 1) * n0.nr * 3,
-                       "per-cell rate-table cotangents", err, errlen);
-  if (rcode) return rcode;
-  cudaStream_t st = (cudaStream_t)stream;
-  cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
-  if (e == cudaSuccess && B > 0) {
-    Net net = s->net;
-    if (rc) net.rc = rc;  // the caller's rate table
-    const CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status,
-                     count, s->list, nullptr};
-    const AdjArgs aa{lm, gx, gh, adapt, stored, gx0, gT, gP, gdt, gh0, glm, s->net.nj > 0 ? gJ : nullptr,
-                     s->vjp_gl, s->vjp_scratch, slot, s->sp_ptr, s->sp_ent, s->st8};
-    s->vjp<<<grid, 32 * WARPS, s->vjp_smem, st>>>(net, a, aa, s->adj_layout);
-    s->vjp_recover<<<rgrid, 32 * WARPS, s->vjp_smem, st>>>(net, a, aa, s->adj_layout, MX_REC_STEPS * max_steps);
-    arrh_kernel<<<n0.nr, ARRH_THREADS, 0, st>>>(net, a, s->vjp_gl, grc);
-    e = cudaGetLastError();
-  } else if (e == cudaSuccess) {
-    e = cudaMemsetAsync(grc, 0, (size_t)n0.nr * 9 * sizeof(double), st);
-  }
-  if (e == cudaSuccess) {
-    add_counts_kernel<<<1, 32, 0, st>>>(count, (long long*)total);
-    e = cudaGetLastError();
-  }
-  if (e != cudaSuccess) {
-    set_error(err, errlen, "mx_vjp: %s", cudaGetErrorString(e));
     return MX_ERR_CUDA;
   }
   return MX_OK;
