@@ -241,3 +241,28 @@ def test_wrong_tangents_are_refused_by_name(case):
                     *(a.expand(17, -1) for a in z[1:]), J=case.t(case.J))  # fmt: skip
     with pytest.raises(ValueError, match="max_steps"):
         case.ad.jvp(x, T, P, dt, h, *z, J=case.t(case.J), max_steps=4001)
+
+
+def test_a_callers_rate_table(gpu, networks):
+    # rc replaces the network's table for the call: ln A of every thermal row moved by 0.1, against the oracle's call
+    # on the same table, and the tangent's and the adjoint's primal alike bit for bit
+    c = Case(networks("cho41"), gpu, cells=64)
+    try:
+        rc = c.cs.tab.rc.copy()
+        rc[: c.cs.tab.nrt, 0] += 0.1
+        z = zeros(c)
+        j = c.ad.jvp(*c.inputs(), *z, rc=c.t(rc), J=c.t(c.J))
+        flag = c.ad.flag.cpu().numpy()
+        v = c.ad.vjp(*c.inputs(), torch.zeros_like(z[0]), rc=c.t(rc), J=c.t(c.J))
+        assert all(torch.equal(a, b) for a, b in zip(j[:4], v[:4]))
+        r = c.o.jvp(c.x, c.T, c.P, c.dt, c.h, rc=rc, J=c.J)
+        same = (j.steps.cpu().numpy() == r["steps"]) & (flag == r["flag"])
+        assert same.mean() >= 0.95
+        a, b = j.x.cpu().numpy()[same], r["x"][same]
+        big = (a > 1e-20) & (b > 1e-20)
+        rel = np.abs(a - b) / np.maximum(a, b).clip(1e-300)
+        assert (np.where(big, rel, 0).max(1) <= 1e-9).mean() >= 0.95 and rel[big].max() <= 1e-6
+        ref = c.cs.launch(*c.inputs(), J=c.t(c.J))
+        assert not torch.equal(ref.x, j.x)  # the table reached the call
+    finally:
+        c.close()
