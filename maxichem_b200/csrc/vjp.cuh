@@ -224,11 +224,16 @@ __device__ __forceinline__ void primal_update(const Net& net, const Cell& c, Ste
 
 // ---- transposed solves (one warp) ----
 
-// y <- M0^-T y with the factors of lu_factor (unit L below the diagonal, U on and above it): U^T z = y ascending,
-// then L^T x = z descending. Row k of the factors is read across the lanes (consecutive addresses).
+// y <- M0^-T y with the factors of lu_factor (unit L below the diagonal, U on and above it), on one warp: U^T z = y in
+// ascending pivots (z_k = a_k / U_kk, then a_i -= U_ki z_k for i > k), then L^T x = z in descending pivots
+// (a_i -= L_ki x_k for i < k). Lane l holds rows l + 32 p; row k of the factors is read across the lanes
+// (consecutive addresses). As lu_solve: pivots 32 at a time, the pivot's value from a register chosen at compile
+// time and one shuffle, and the next row loaded while the current pivot is applied; a lane whose row takes no update
+// from pivot k uses the multiplier 0 (fma(-0, z, a) = a for finite z). Each entry takes the one-pivot sweep's fma's in
+// its order.
 template <int R>
-__device__ void lu_solve_t(const Net& net, const double* A, const double* dinv, double* y, int lane) {
-  const int ns = net.ns, ld = net.ld;
+__device__ __noinline__ void lu_solve_t(const Net& net, const double* A, const double* dinv, double* y, int lane) {
+  const int ns = net.ns, ld = net.ld, last = ns - 1;
   double a[R], d[R];
 #pragma unroll
   for (int p = 0; p < R; p++) {
@@ -236,25 +241,47 @@ __device__ void lu_solve_t(const Net& net, const double* A, const double* dinv, 
     a[p] = i < ns ? y[i] : 0.0;
     d[p] = i < ns ? dinv[i] : 0.0;
   }
-  for (int k = 0; k < ns; k++) {
-    const int pk = k >> 5;
-    const double zk = __shfl_sync(FULL, pick<R>(a, pk) * pick<R>(d, pk), k & 31);
-    const double* row = A + k * ld;
 #pragma unroll
-    for (int p = 0; p < R; p++) {
-      const int i = lane + 32 * p;
-      if (i == k) a[p] = zk;
-      else if (i > k && i < ns) a[p] = fma(-row[i], zk, a[p]);
+  for (int c = 0; c < R; c++) {  // U^T: pivots 32c .. 32c + 31
+    const int k0 = 32 * c, k1 = min(k0 + 32, ns);
+    if (k0 >= k1) break;
+    double m[R];
+#pragma unroll
+    for (int p = c; p < R; p++) m[p] = A[k0 * ld + min(lane + 32 * p, last)];
+#pragma unroll 2
+    for (int k = k0; k < k1; k++) {
+      const double zk = __shfl_sync(FULL, a[c] * d[c], k & 31);
+      if (lane == (k & 31)) a[c] = zk;
+      double mn[R];
+#pragma unroll
+      for (int p = c; p < R; p++) mn[p] = A[min(k + 1, last) * ld + min(lane + 32 * p, last)];
+#pragma unroll
+      for (int p = c; p < R; p++) {
+        const bool act = (p > c ? true : lane > k - k0) && lane + 32 * p < ns;
+        a[p] = fma(-(act ? m[p] : 0.0), zk, a[p]);
+        m[p] = mn[p];
+      }
     }
   }
-  for (int k = ns - 1; k > 0; k--) {
-    const int pk = k >> 5;
-    const double xk = __shfl_sync(FULL, pick<R>(a, pk), k & 31);
-    const double* row = A + k * ld;
 #pragma unroll
-    for (int p = 0; p < R; p++) {
-      const int i = lane + 32 * p;
-      if (i < k) a[p] = fma(-row[i], xk, a[p]);
+  for (int c = R - 1; c >= 0; c--) {  // L^T: pivots 32c + 31 .. 32c (down to 1)
+    const int k0 = 32 * c, khi = min(k0 + 31, last), klo = max(k0, 1);
+    if (khi < klo) continue;
+    double m[R];
+#pragma unroll
+    for (int p = 0; p <= c; p++) m[p] = A[khi * ld + min(lane + 32 * p, last)];
+#pragma unroll 2
+    for (int k = khi; k >= klo; k--) {
+      const double xk = __shfl_sync(FULL, a[c], k & 31);
+      double mn[R];
+#pragma unroll
+      for (int p = 0; p <= c; p++) mn[p] = A[max(k - 1, 0) * ld + min(lane + 32 * p, last)];
+#pragma unroll
+      for (int p = 0; p <= c; p++) {
+        const bool act = p < c ? true : lane < k - k0;
+        a[p] = fma(-(act ? m[p] : 0.0), xk, a[p]);
+        m[p] = mn[p];
+      }
     }
   }
   __syncwarp();
