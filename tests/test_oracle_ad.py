@@ -178,3 +178,31 @@ def test_no_multipliers_are_zero_multipliers(case):
     for k in ("x", "h", "steps", "dx", "dh"):
         assert np.array_equal(none[k], zero[k]), k
     assert np.abs(none["dx"]).max() > 0.0
+
+
+@pytest.fixture(scope="module")
+def recovered():
+    # cold starts with max_steps 20: the call leaves them unfinished, the guard lists them, and the recovery (dense
+    # pivoted W, ten times the tries) redoes them, so the tangent runs along the recovery's path
+    net = synthetic.network("cho41")
+    tab = tables.build(net, True, warps=4)
+    w = synthetic.workload(net, "column", 64, seed=3)
+    x, h, _ = synthetic.cold_start(w.x, w.h, seed=4, share=0.3)
+    sel = np.arange(0, 64, 4)
+    rng = np.random.default_rng(5)
+    return {
+        "o": Oracle(tab), "tab": tab, "x": x[sel], "T": w.T[sel], "P": w.P[sel], "dt": np.full(len(sel), 100.0),
+        "h": h[sel], "J": w.J[sel], "lm": 0.1 * rng.standard_normal((len(sel), tab.nr)),
+    }  # fmt: skip
+
+
+@pytest.mark.parametrize("cls", ["x", "T", "lm", "rc"])
+def test_recovered_tangent_against_differences(recovered, cls, monkeypatch):
+    o = recovered["o"]
+    jvp = o.jvp
+    monkeypatch.setattr(o, "jvp", lambda *a, **k: jvp(*a, max_steps=20, **k))
+    errors, judged, r = _tangent_case(recovered, cls, 13)
+    assert (r["flag"] == 1).sum() >= 12, r["flag"]
+    fin = errors[np.isfinite(errors)]
+    assert len(fin) >= FD_COVERAGE * judged and judged >= 8, (cls, len(fin), judged)
+    assert np.quantile(fin, 0.9) <= FD_P90 and fin.max() <= FD_MAX, (cls, np.quantile(fin, 0.9), fin.max())
