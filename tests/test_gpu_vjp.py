@@ -292,3 +292,34 @@ def test_long_dark_calls(gpu, networks, adapt):
             assert (e <= bound).all(), (cls, e[e > bound], floors[cls][e > bound])
     finally:
         c.close()
+
+
+def test_without_photolysis(gpu, networks):
+    # photo=False: no photolysis branches, J None, no J cotangent; the primal is still the call's bit for bit and the
+    # adjoint still the tangent's transpose
+    net = networks("cho41")
+    cs, ad = CudaSolver(net, gpu), ADSolver(net, gpu)
+    try:
+        B = 32
+        w = synthetic.workload(net, "column", B, seed=7)
+        x, h, _ = synthetic.cold_start(w.x, w.h, seed=8, share=0.3)
+        t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=gpu)  # noqa: E731
+        args = [t(x), t(w.T), t(w.P), t(np.full(B, 100.0)), t(h)]
+        ref = cs.launch(*args)
+        rng = np.random.default_rng(3)
+        dx, dT = x * rng.standard_normal(x.shape), w.T * rng.standard_normal(B)
+        zero = t(np.zeros(B))
+        j = ad.jvp(*args, t(dx), t(dT), zero, zero, zero)
+        assert all(torch.equal(a, b) for a, b in zip(ref[:4], j[:4]))
+        x1 = j.x.cpu().numpy()
+        c = np.where(x1 > 1e-20, rng.standard_normal(x1.shape) / np.maximum(x1, 1e-300), 0.0)
+        v = ad.vjp(*args, t(c))
+        assert v.cotangents.J is None and all(torch.equal(a, b) for a, b in zip(ref[:4], v[:4]))
+        g = v.cotangents
+        left = (c * j.dx.cpu().numpy()).sum(1)
+        right = (g.x.cpu().numpy() * dx).sum(1) + g.T.cpu().numpy() * dT
+        e = np.abs(left - right) / np.maximum(np.abs(left), np.abs(right)).clip(1e-300)
+        assert np.quantile(e, 0.99) <= DOT_P99 and e.max() <= DOT_MAX, e.max()
+    finally:
+        cs.close()
+        ad.close()
