@@ -206,3 +206,18 @@ def test_recovered_tangent_against_differences(recovered, cls, monkeypatch):
     fin = errors[np.isfinite(errors)]
     assert len(fin) >= FD_COVERAGE * judged and judged >= 8, (cls, len(fin), judged)
     assert np.quantile(fin, 0.9) <= FD_P90 and fin.max() <= FD_MAX, (cls, np.quantile(fin, 0.9), fin.max())
+
+
+def test_frozen_contract_has_no_dt_or_h_tangent(case):
+    # the frozen contract holds every accepted try's size: neither dt nor the starting step reaches x or h_out
+    o = case["o"]
+    x, T, P, dt, h, J = (case[k] for k in ("x", "T", "P", "dt", "h", "J"))
+    B, ns = x.shape
+    rng = np.random.default_rng(6)
+    r = o.jvp(x, T, P, dt, h, np.zeros((2, B, ns)), np.zeros((2, B)), np.zeros((2, B)),
+              np.stack([dt * rng.standard_normal(B), np.zeros(B)]), np.stack([np.zeros(B), h * rng.standard_normal(B)]),
+              J=J, adapt=False)  # fmt: skip
+    assert (r["dx"] == 0.0).all() and (r["dh"] == 0.0).all()
+    a = o.jvp(x, T, P, dt, h, np.zeros((1, B, ns)), np.zeros((1, B)), np.zeros((1, B)),
+              (dt * rng.standard_normal(B))[None], np.zeros((1, B)), J=J)  # fmt: skip
+    assert np.abs(a["dx"]).max() > 0.0  # the adaptive contract has one
