@@ -48,7 +48,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--cells", type=int, default=1 << 20, help="cells per GPU")
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--cpu-sample", type=int, default=262144, help="cells of the CPU baseline sample")
-    p.add_argument("--ref-sample", type=int, default=16384,
+    p.add_argument("--ref-sample", type=int, default=32768,
                    help="cells of the reference arm's sample (its four spin-up calls run on the CPU too)")
     p.add_argument("--workload", choices=("column", "uneven"), default="column",
                    help="uneven: 262,144 cells, half at night, a quarter cold starts, a loop of --calls calls")
@@ -125,15 +125,18 @@ def run_reference(args) -> None:
     tab = tables.build(net, True)
     ref = oracle.Oracle(tab)
     sample = min(args.ref_sample, args.cells)
-    w = inputs(net, sample, seed=7)
-    x, h = w.x, w.h
+    # the GPU arm's own cells (rank 0's seed, the full batch's column grid), the first `sample` of them (whole columns)
+    w = inputs(net, args.cells, seed=1000)
+    w.dt[:] = args.dt
+    T, P, dt, J = w.T[:sample], w.P[:sample], w.dt[:sample], w.J[:sample]
+    x, h = w.x[:sample], w.h[:sample]
     for _ in range(SPINUP_CALLS):
-        r = ref.call(x, w.T, w.P, w.dt, h, J=w.J)
+        r = ref.call(x, T, P, dt, h, J=J)
         x, h = r["x"], r["h"]
     times = []
     for k in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        ref.call(x, w.T, w.P, w.dt, h, J=w.J)
+        ref.call(x, T, P, dt, h, J=J)
         if k >= args.warmup:
             times.append(time.perf_counter() - t0)
     value = sample / float(np.mean(times))
@@ -142,20 +145,49 @@ def run_reference(args) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{NETWORK} column grid, call {SPINUP_CALLS + 1} of 300 s calls", "cells": sample,
-                   "species": tab.ns, "reactions": tab.nr},
+        "config": {"workload": f"{NETWORK}: call {SPINUP_CALLS + 1} of {args.dt:g} s calls on a {LEVELS}-level "
+                               "column grid",
+                   "cells": sample, "species": tab.ns, "reactions": tab.nr,
+                   "sample_of": f"the first {sample} of the GPU arm's {args.cells} cells (seed 1000, whole columns)"},
         "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "port",
-                         "sample": f"{sample} cells of the same call, all {cores} host threads (OpenMP)"},
+                         "sample": f"the first {sample} cells of the same call (its four spin-up calls also on the "
+                                   f"CPU), all {cores} host threads (OpenMP)"},
         "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }  # fmt: skip
     print(json.dumps(line), flush=True)
 
 
+def launch_ranks(args) -> None:
+    """--gpus N > 1 outside torchrun: start N ranks of this script under torch.distributed.run (one per GPU) and exit
+    with their status; inside torchrun, the world size must be N. Fails clearly when fewer GPUs are visible."""
+    from maxichem_b200 import replicas
+
+    if replicas.under_launcher():
+        world = int(os.environ["WORLD_SIZE"])
+        if world != args.gpus:
+            sys.exit(f"bench.py --gpus {args.gpus} runs under a launcher of {world} ranks: they must agree")
+        return
+    if args.gpus <= 1:
+        return
+    import torch
+
+    visible = torch.cuda.device_count() if torch.cuda.is_available() else 0
+    if visible < args.gpus:
+        sys.exit(f"bench.py --gpus {args.gpus}: only {visible} CUDA devices are visible; one rank per GPU needs "
+                 f"{args.gpus}")  # fmt: skip
+    os.environ.setdefault("NCCL_DEBUG", "INFO")  # the ranks' NCCL init lines show the communicator's size
+    os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+    sys.exit(replicas.relaunch(args.gpus, str(Path(__file__).resolve()), sys.argv[1:]))
+
+
 def main() -> None:
     args = parse()
+    if args.gpus < 1:
+        sys.exit(f"bench.py --gpus: at least 1 expected, got {args.gpus}")
     if args.impl == "reference":
         run_reference(args)
         return
+    launch_ranks(args)
     if args.workload == "uneven":
         run_uneven(args)
         return
@@ -388,7 +420,7 @@ def run_uneven(args) -> None:
     cl = graph.CallLoop(solver, x0, T, P, dt, h0, J=J, calls=args.calls)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    last = cl.run()
+    last = cl.run(check=False)
     e1.record(stream)
     e1.synchronize()
     graph_ms = e0.elapsed_time(e1)

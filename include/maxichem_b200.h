@@ -145,8 +145,9 @@ int mx_call(mx_solver* s, const double* x, const double* T, const double* P, con
  * entries instead of solver-owned memory, so the call never calls cudaMalloc, cudaFree or any allocating library
  * routine (the solver handle itself still comes from mx_create, once, at set-up).
  * - B above MX_STATIC_MAX_CELLS is refused with MX_ERR_ARGUMENT and a message naming the limit.
- * - The first call on a device looks up the array's address there (cudaGetSymbolAddress, with that device current)
- *   and keeps it; make that first call before any stream capture on the device.
+ * - Each call looks up the array's address on the solver's device (cudaGetSymbolAddress, with that device current)
+ *   and passes it to the kernels: the array's name is only a host-side stand-in in host code. The first call on a
+ *   device may load the library's module there; make that first call before any stream capture on the device.
  * - Every call of every solver in the process shares the array, which keeps the last call's contents. Nothing in it
  *   must start at zero (a call writes each entry before reading it); the queue and list counters that must start at
  *   zero are in count, which the call clears. Calls that overlap on the GPU (other streams, other threads) race on
@@ -213,7 +214,7 @@ int mx_guard(mx_solver* s, const double* x, double* x_out, const int32_t* done, 
 
 /* Launch layout of the solver, for reports: warps per cell, rows per lane of the solves, shared bytes per cell,
  * call and recovery CTAs per SM at full occupancy, SMs, the matrix's leading dimension, the call grid's CTAs per SM
- * (0: one CTA per cell). */
+ * (0: one CTA per cell), the cells the solver-owned recompute list holds (0 until an mx_call or mx_guard sized it). */
 int mx_info(const mx_solver* s, int32_t* values, int32_t n);
 
 /* The call kernel's grid for later calls: ctas_per_sm from 1 to the occupancy limit runs that many persistent CTAs per

@@ -11,7 +11,6 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <new>
 #include <vector>
 
@@ -744,6 +743,10 @@ extern "C" int mx_call(mx_solver* s, const double* x, const double* T, const dou
     return MX_ERR_ARGUMENT;
   }
   DeviceScope scope(s->device);
+  if (scope.status != cudaSuccess) {
+    set_error(err, errlen, "mx_call: device %d: %s", s->device, cudaGetErrorString(scope.status));
+    return MX_ERR_CUDA;
+  }
   cudaStream_t st = (cudaStream_t)stream;
   int rc = grow_list(s, std::max<int64_t>(B, 1), err, errlen);
   if (rc) return rc;
@@ -803,7 +806,7 @@ extern "C" int mx_guard(mx_solver* s, const double* x, double* x_out, const int3
 extern "C" int mx_info(const mx_solver* s, int32_t* values, int32_t n) {
   if (!s || !values) return MX_ERR_ARGUMENT;
   const int32_t v[] = {WARPS, s->rows_per_lane, (int32_t)s->smem, s->call_ctas, s->recover_ctas, s->sms, s->net.ld,
-                       s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas};
+                       s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas, (int32_t)s->list_capacity};
   for (int i = 0; i < n && i < (int)(sizeof v / sizeof v[0]); i++) values[i] = v[i];
   return MX_OK;
 }
@@ -899,35 +902,24 @@ extern "C" int mx_probe_fp64(int device, int64_t iters, double* gflops) {
 // ---- mx_call_static: the call for callers that cannot allocate device memory ----
 // For a GCM whose framework holds the GPU's memory in its own pool, or whose time loop must not pay the device-wide
 // synchronisation of cudaMalloc and cudaFree. The only scratch a call owns is the recompute list (one int per cell).
-// Here it is a file-scope device array of
-// MX_STATIC_MAX_CELLS entries that every mx_call_static call shares; its address on a device is looked up once, at
-// that device's first call, with the device current.
+// Here it is a file-scope device array of MX_STATIC_MAX_CELLS entries that every mx_call_static call shares. In host
+// code its name stands for a host-side shadow, not a device address, so each call looks up its address on the
+// solver's device (cudaGetSymbolAddress, with that device current) and passes that to the kernels. Looking it up on
+// every call, rather than caching it per device, keeps it right after a cudaDeviceReset or under another context.
 
 static __device__ __align__(256) int g_static_list[MX_STATIC_MAX_CELLS];
 
 namespace {
 
-constexpr int MAX_DEVICES = 64;
-int* g_static_list_ptr[MAX_DEVICES] = {};
-std::mutex g_static_mutex;
-
 int static_list(int device, int** out, char* err, size_t errlen) {
-  if (device < 0 || device >= MAX_DEVICES) {
-    set_error(err, errlen, "mx_call_static: device %d out of range", device);
-    return MX_ERR_ARGUMENT;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_static_list);
+  if (e != cudaSuccess || !p) {
+    set_error(err, errlen, "mx_call_static: the static scratch's address on device %d: %s", device,
+              cudaGetErrorString(e));
+    return MX_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lock(g_static_mutex);
-  if (!g_static_list_ptr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_list);
-    if (e != cudaSuccess || !p) {
-      set_error(err, errlen, "mx_call_static: the static scratch's address on device %d: %s", device,
-                cudaGetErrorString(e));
-      return MX_ERR_CUDA;
-    }
-    g_static_list_ptr[device] = static_cast<int*>(p);
-  }
-  *out = g_static_list_ptr[device];
+  *out = static_cast<int*>(p);
   return MX_OK;
 }
 

@@ -3,14 +3,16 @@
 A GCM advances the same cells call after call: call k + 1 starts from call k's x and h, with the column's T, P, dt
 and J of that step. ``CallLoop`` captures `calls` such calls (the call, recovery and count kernels of each, with
 their count resets) in one CUDA graph, so a replay launches the whole loop with one host call and no host
-synchronisation in between; the refusal check the Python call makes after every call is made once, on the counts
-the loop added to ``solver.total``. Outputs alternate between two sets of buffers.
+synchronisation in between; the refusal check the Python call makes after every call is made once per replay, on the
+counts the loop added to ``solver.total`` (``run(check=True)``, one small read-back after the replay). Outputs
+alternate between two sets of buffers.
 """
 
 from __future__ import annotations
 
 import torch
 
+from .constants import COUNTS
 from .solver import CudaSolver, check_inputs, check_photolysis
 
 
@@ -57,10 +59,29 @@ class CallLoop:
         return {"x": torch.empty(B, ns, dtype=torch.float64, device=dev), "h": f, "steps": torch.empty_like(f),
                 **{k: torch.empty(B, dtype=torch.int32, device=dev) for k in ("done", "flag", "status")}}  # fmt: skip
 
-    def run(self) -> dict[str, torch.Tensor]:
-        """Replay the loop on torch's current stream; return the last call's outputs (buffers of the loop)."""
+    def run(self, check: bool = True) -> dict[str, torch.Tensor]:
+        """Replay the loop on torch's current stream; return the last call's outputs (buffers of the loop).
+
+        With ``check`` the counts the replay added to ``solver.total`` are read back once (the loop's one host
+        synchronisation) and ValueError is raised if any call of the loop refused a cell (bad input, or T outside
+        the solver's range), as the Python call does after each call. ``check=False`` leaves the replay
+        asynchronous (for timing); ``refused`` then reads the counts later."""
+        before = self.solver.total.clone() if check else None
         self.graph.replay()
+        if check:
+            refused = self.refused(before)
+            if any(refused.values()):
+                raise ValueError(
+                    "the call loop refused cells: "
+                    + ", ".join(f"{n} {kind}" for kind, n in refused.items() if n)
+                    + f" over its {self.calls} calls (cell-calls); check the loop's inputs with a plain call"
+                )
         return self.last
+
+    def refused(self, before: torch.Tensor) -> dict[str, int]:
+        """Refused cell-calls (bad_input, cold, hot) added to ``solver.total`` since it held ``before``."""
+        added = (self.solver.total - before).tolist()
+        return {kind: int(added[1 + COUNTS.index(kind)]) for kind in ("bad_input", "cold", "hot")}
 
     def carry(self) -> None:
         """Make the last call's x and h the next run's starting state."""

@@ -10,6 +10,9 @@ may add up their counts (SUM). Both are one small collective on the process grou
 from __future__ import annotations
 
 import os
+import socket
+import subprocess
+import sys
 from typing import NamedTuple
 
 import torch
@@ -65,3 +68,31 @@ def sum_counts(total: torch.Tensor) -> torch.Tensor:
 def throughput(cells_per_rank: int, world: int, seconds: float) -> float:
     """Whole-job cells/s: the cells of all ranks over the slowest rank's time."""
     return world * cells_per_rank / seconds
+
+
+def free_port() -> int:
+    """A free TCP port on 127.0.0.1 for a rendezvous."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return int(s.getsockname()[1])
+
+
+def under_launcher() -> bool:
+    """True in a rank that torchrun (torch.distributed.run) started."""
+    return "RANK" in os.environ and "WORLD_SIZE" in os.environ
+
+
+def torchrun_command(n: int, script: str, argv: list[str], port: int | None = None) -> list[str]:
+    """The command that runs ``script argv`` as n ranks of one node under torch.distributed.run, with the rendezvous on
+    127.0.0.1 (the host name may not resolve)."""
+    if n < 1:
+        raise ValueError(f"ranks: at least 1 expected, got {n}")
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", str(n),
+            "--master-addr", "127.0.0.1", "--master-port", str(port or free_port()), script, *argv]  # fmt: skip
+
+
+def relaunch(n: int, script: str, argv: list[str], timeout: float | None = None) -> int:
+    """Run ``script argv`` as n ranks under torch.distributed.run and wait for them; return the launcher's exit code
+    (non-zero when a rank failed). Each rank reads its rank and world size from the environment (rank_from_env)."""
+    proc = subprocess.run(torchrun_command(n, script, argv), timeout=timeout)
+    return proc.returncode

@@ -26,7 +26,7 @@ __all__ = ["ATOL", "COUNTS", "DRIFT", "REC_STEPS", "T_MAX", "T_MIN", "X_SUM_TOL"
 
 _ERRLEN = 1024
 INFO_FIELDS = ("warps", "rows_per_lane", "smem", "call_ctas_per_sm", "recover_ctas_per_sm", "sms", "ld",
-               "grid_ctas_per_sm")
+               "grid_ctas_per_sm", "list_cells")
 
 
 class CallResult(NamedTuple):
@@ -248,7 +248,14 @@ class CudaSolver:
             )
         values = (ctypes.c_int32 * len(INFO_FIELDS))()
         self._lib.mx_info(self._handle, values, len(INFO_FIELDS))
-        self.info["grid_ctas_per_sm"] = int(values[len(INFO_FIELDS) - 1])
+        self.info["grid_ctas_per_sm"] = int(values[INFO_FIELDS.index("grid_ctas_per_sm")])
+
+    def layout(self) -> dict[str, int]:
+        """The library's current launch layout (mx_info), read afresh: ``info``'s fields as they are now."""
+        self._require_open()
+        values = (ctypes.c_int32 * len(INFO_FIELDS))()
+        self._lib.mx_info(self._handle, values, len(INFO_FIELDS))
+        return dict(zip(INFO_FIELDS, list(values)))
 
     def call_host(self, x: torch.Tensor, T: torch.Tensor, P: torch.Tensor, dt: torch.Tensor, h: torch.Tensor, *,
                   rtol: float = DEFAULT_RTOL, atol: float = ATOL, max_steps: int = DEFAULT_MAX_STEPS,

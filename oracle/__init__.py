@@ -20,7 +20,10 @@ from maxichem_b200.tables import Tables
 HERE = Path(__file__).resolve().parent
 SOURCES = [HERE / "mx_oracle.c", HERE / "mx_oracle_ad.c"]
 LIBRARY = HERE / "_build" / "libmx_oracle.so"
-FLAGS = ["-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-std=c11", "-Wall"]
+# -O3 with the x86-64-v3 level (AVX2, BMI2) rather than -march=native: the built library travels to machines whose
+# CPUs may differ from the build machine's; -ffp-contract=off keeps every multiply-add unfused unless written as fma.
+FLAGS = ["-O3", "-march=x86-64-v3", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
+         "-std=c11", "-Wall"]  # fmt: skip
 
 _lib: ctypes.CDLL | None = None
 

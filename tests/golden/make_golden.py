@@ -1,9 +1,9 @@
 """Write the golden fixtures of tests/golden from the reference implementation (imalsky/maxichem).
 
-Run in a container that has the reference checked out (read-only) at REFERENCE below; the fixtures it writes are
-committed, so the tests never need the reference itself:
+Run where the reference is checked out (read-only is enough), with its path as the one argument; the fixtures it
+writes are committed, so the tests never need the reference itself:
 
-  python tests/golden/make_golden.py [/path/to/reference]
+  python tests/golden/make_golden.py /path/to/reference
 
 * reader.json / reader.npz: the reference reader's VulcanNetwork of each synthetic network (species, elements,
   S, Sp, atoms, NASA-9 ranges, reaction dicts);
@@ -29,7 +29,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REFERENCE = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if len(sys.argv) != 2 or not (Path(sys.argv[1]) / "maxichem").is_dir():
+    sys.exit("usage: python tests/golden/make_golden.py /path/to/reference  (a checkout of imalsky/maxichem)")
+REFERENCE = Path(sys.argv[1])
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(REFERENCE))
 sys.path.insert(0, str(REFERENCE / "tests"))

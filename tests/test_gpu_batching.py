@@ -84,3 +84,17 @@ def test_a_captured_loop_equals_the_calls_one_by_one(uneven):
     loop.carry()
     assert torch.equal(loop.x_in, outs[-1]["x"]) and torch.equal(loop.h_in, outs[-1]["h"])
     loop.close()
+
+
+def test_a_captured_loop_refuses_a_cold_cell(uneven):
+    solver, (x, T, P, dt, h, J), _ = uneven
+    n = 256
+    T2 = T[:n].clone()
+    T2[5] = 250.0  # below the solver's range: every call of the loop refuses it
+    loop = graph.CallLoop(solver, x[:n], T2, P[:n], dt[:n], h[:n], J=J[:n], calls=2)
+    with pytest.raises(ValueError, match=r"the call loop refused cells: 2 cold over its 2 calls"):
+        loop.run()
+    before = solver.total.clone()
+    loop.run(check=False)
+    assert loop.refused(before) == {"bad_input": 0, "cold": 2, "hot": 0}
+    loop.close()

@@ -91,3 +91,47 @@ def test_two_gloo_ranks_agree_on_time_counts_and_results(tmp_path, networks):
     per_rank = np.sum([p["count"] for p in got["parts"]], axis=0)
     assert got["counts"] == per_rank.tolist()
     assert got["counts"][1:-1] == whole["count"][1:-1].tolist()
+
+
+RANK_SCRIPT = """
+import datetime, json, sys
+import torch
+import torch.distributed as dist
+sys.path.insert(0, {root!r})
+from maxichem_b200 import replicas
+rank, local, world = replicas.rank_from_env()
+dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+ms = replicas.max_over_ranks(10.0 + rank, torch.device("cpu"))
+counts = replicas.sum_counts(torch.full((12,), rank + 1, dtype=torch.int64))
+if rank == 0:
+    open(sys.argv[1], "w").write(json.dumps({{"world": world, "ms": ms, "counts": counts.tolist(),
+                                              "value": replicas.throughput(1000, world, ms * 1e-3)}}))
+dist.destroy_process_group()
+"""
+
+
+def test_the_launcher_starts_the_ranks_and_they_take_the_slowest_time(tmp_path):
+    script = tmp_path / "rank.py"
+    script.write_text(RANK_SCRIPT.format(root=str(ROOT)))
+    out = tmp_path / "out.json"
+    cmd = replicas.torchrun_command(2, str(script), [str(out)], port=1234)
+    assert cmd[1:9] == ["-m", "torch.distributed.run", "--nnodes", "1", "--nproc-per-node", "2", "--master-addr",
+                        "127.0.0.1"]  # fmt: skip
+    assert replicas.relaunch(2, str(script), [str(out)], timeout=240) == 0
+    got = json.loads(out.read_text())
+    assert got["world"] == 2 and got["ms"] == 11.0 and got["counts"] == [3] * 12
+    assert got["value"] == 2 * 1000 / 11e-3
+
+
+def test_bench_refuses_more_gpus_than_are_visible():
+    import subprocess
+
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("checks the refusal on a machine without enough GPUs")
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2"], capture_output=True, text=True,
+                       timeout=300, env=env)  # fmt: skip
+    assert r.returncode != 0
+    assert "bench.py --gpus 2: only 0 CUDA devices are visible" in r.stderr
