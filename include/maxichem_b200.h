@@ -158,6 +158,37 @@ int mx_call_static(mx_solver* s, const double* x, const double* T, const double*
                    double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag, int32_t* status,
                    int32_t* count, int64_t* total, void* stream, char* err, size_t errlen);
 
+/* Precisions of mx_set_precision. */
+#define MX_PRECISION_FP64 0
+#define MX_PRECISION_MIXED 1
+#define MX_MIXED_MAX_SWEEPS 4
+/* The mixed path's default trust bound: a try whose last refinement moved a stage vector by more than this share of
+ * the error-control scale (rtol |N| + atol) has its cell redone in FP64. */
+#define MX_MIXED_TOL 1.0
+
+/*
+ * The arithmetic of later mx_call calls of this solver (north-star form 1; no counterpart in the reference, whose
+ * solve is FP64 throughout). MX_PRECISION_FP64 (the default): the plain path. MX_PRECISION_MIXED: each try's matrix
+ * M0 = I / (gamma h) - Jn is row-scaled by powers of two, factored in FP32 and every stage solve is refined `sweeps`
+ * times (1..MX_MIXED_MAX_SWEEPS) against an FP64 residual formed from the rate tables (no FP64 matrix is stored);
+ * rates, equilibrium constants, right-hand sides, stage vectors, the error estimate, step control and the guard stay
+ * FP64. A try whose last correction exceeds tol (> 0) times the error-control scale hands its cell to the plain FP64
+ * kernel, which redoes it from its inputs in the same call. Results, counts and flags have mx_call's meaning.
+ * mx_call_static always runs the plain path.
+ */
+int mx_set_precision(mx_solver* s, int32_t precision, int32_t sweeps, double tol);
+
+/* Register a device int64[1] that later mixed-precision calls add the number of cells they handed to the FP64 kernel
+ * to (NULL stops counting). No counterpart in the reference. */
+int mx_set_escalation_counter(mx_solver* s, int64_t* counter);
+
+/* One fresh try of one cell (device x [ns], J [nj]) at try size h through the mixed path with `sweeps` refinements
+ * (0..MX_MIXED_MAX_SWEEPS): out = K1, K2, K3, K4, N' [ns each, elimination order], err, ok, the largest last
+ * correction and the largest first correction on the error-control scale. No counterpart in the reference: a test
+ * hook, against mx_debug_try's FP64 stages. */
+int mx_debug_try_mixed(mx_solver* s, const double* x, double T, double P, double h, const double* J, double rtol,
+                       double atol, int32_t sweeps, double* out, void* stream);
+
 /* Tangent directions of one mx_jvp call at most (the reference's DMAX, maxichem/_constants.py:29). */
 #define MX_JVP_MAX_DIRECTIONS 16
 
@@ -214,12 +245,14 @@ int mx_guard(mx_solver* s, const double* x, double* x_out, const int32_t* done, 
 
 /* Launch layout of the solver, for reports: warps per cell, rows per lane of the solves, shared bytes per cell,
  * call and recovery CTAs per SM at full occupancy, SMs, the matrix's leading dimension, the call grid's CTAs per SM
- * (0: one CTA per cell), the cells the solver-owned recompute list holds (0 until an mx_call or mx_guard sized it). */
+ * (0: one CTA per cell), the cells the solver-owned recompute list holds (0 until an mx_call or mx_guard sized it),
+ * the mixed kernel's shared bytes per cell and CTAs per SM, the precision (MX_PRECISION_*) and refinement sweeps. */
 int mx_info(const mx_solver* s, int32_t* values, int32_t n);
 
-/* The call kernel's grid for later calls: ctas_per_sm from 1 to the occupancy limit runs that many persistent CTAs per
- * SM over the cell queue; 0 launches one CTA per cell (a static launch); -1 restores the default (the occupancy
- * limit). Results do not depend on it. No counterpart in the reference, which picks its cells per block by
+/* The call kernel's grid for later calls: ctas_per_sm from 1 to the occupancy limit (the larger of the plain and the
+ * mixed kernel's; each kernel takes at most its own) runs that many persistent CTAs per SM over the cell queue; 0
+ * launches one CTA per cell (a static launch); -1 restores the default (the occupancy limit). Results do not depend
+ * on it. No counterpart in the reference, which picks its cells per block by
  * recompiling (maxichem/kincuda.py:184-218); maxichem_b200/autotune.py times the choices. */
 int mx_set_grid(mx_solver* s, int32_t ctas_per_sm);
 
@@ -269,6 +302,83 @@ int mx_mass_to_mole(const double* q, const double* mw, int64_t B, int32_t ns, in
                     int32_t* bad, void* stream);
 int mx_mole_to_mass(const double* x, const double* mw, const double* mass, int64_t B, int32_t ns, double* q,
                     int32_t* bad, void* stream);
+
+/*
+ * The learned part of the call (north-star form 4; no counterpart in the reference). A BF16 MLP surrogate of the
+ * per-call solve: features of a cell (log10 x per species floored at 1e-30, log10 T, P and dt, log10(J + 1e-30) per
+ * branch, standardised, zero-padded to a multiple of 64: kin) -> `layers` hidden layers of width `hidden` (SiLU) ->
+ * `heads` output blocks of nt = ns + 1 values (log10 x_out - log10 x_in per species, log10 h_out; standardised),
+ * padded to kout (a multiple of 64). Every layer is a tcgen05 GEMM with its bias and activation fused; training on
+ * the GPU by the same GEMMs (backward dX with the SiLU derivative fused, dW), bias sums and Adam.
+ */
+typedef struct mx_surrogate mx_surrogate;
+
+/* A surrogate for a network of ns species, nj photolysis branches and nel elements (atoms [ns][nel], host, network
+ * order), with zero weights and unit scaling, on one device. */
+int mx_sur_create(int32_t ns, int32_t nj, int32_t nel, const double* atoms, int32_t hidden, int32_t layers,
+                  int32_t heads, int32_t device, mx_surrogate** out, char* err, size_t errlen);
+
+/* Sizes: nf (features), kin, nt, kout, P (FP32 parameters), layers, hidden, heads, training steps taken. */
+int mx_sur_info(const mx_surrogate* s, int64_t* values, int32_t n);
+
+/* The standardisation (host float arrays): feature mean, deviation and training range [lo, hi] ([nf] each), target
+ * mean and deviation ([nt] each). A cell with a feature outside its range is never accepted. */
+int mx_sur_set_scaling(mx_surrogate* s, const float* feat_mean, const float* feat_std, const float* feat_lo,
+                       const float* feat_hi, const float* tgt_mean, const float* tgt_std);
+
+/* Features of B cells (device inputs as mx_call's) into feat (device BF16 [B][kin]) and in_range (device int32 [B],
+ * nullable: 1 when every feature is inside the training range). Asynchronous on stream. */
+int mx_sur_features(mx_surrogate* s, const double* x, const double* T, const double* P, const double* dt,
+                    const double* J, int64_t B, void* feat, int32_t* in_range, void* stream);
+
+/* The network on B rows of features (device BF16 [B][kin]) into pred (device FP32 [B][kout]), in chunks of 65,536
+ * rows. Asynchronous on stream. */
+int mx_sur_forward(mx_surrogate* s, const void* feat, int64_t B, float* pred, void* stream);
+
+/* One Adam step (lr, betas 0.9 / 0.999, eps 1e-8) on a batch of M rows (a multiple of 64): features feat (BF16
+ * [M][kin]), standardised targets tgt (FP32 [M][nt]) and per-row head weights wts (FP32 [M][heads], the heads'
+ * bootstrap draw). The loss is the weighted mean square error over rows, heads and targets; *loss (device FP32,
+ * nullable) is incremented by it. Asynchronous on stream; lr 0 computes the gradients only (mx_sur_params 1). */
+int mx_sur_train_step(mx_surrogate* s, const void* feat, const float* tgt, const float* wts, int64_t M, float lr,
+                      float* loss, void* stream);
+
+/* The FP32 parameters (which 0) or the last step's gradients (which 1) into a host array of P floats, layer by layer:
+ * W_l [out][in] then b_l [out]. Synchronises. mx_sur_set_params writes them (and restarts Adam). */
+int mx_sur_params(mx_surrogate* s, int32_t which, float* host, int64_t n);
+int mx_sur_set_params(mx_surrogate* s, const float* host, int64_t n);
+
+/* The GEMMs' error flag (1 when a wait on the tensor-core pipeline gave up), read and cleared. Synchronises. */
+int mx_sur_error(mx_surrogate* s, int32_t* flag);
+
+/*
+ * The gated call: for B cells (device arrays as mx_call's) the network proposes each cell's end-of-call state (the
+ * heads' mean) and step size. A proposal is accepted only if every feature is inside the training range, the heads'
+ * largest deviation over species above 1e-20 is at most spread_max (dex), and projecting it onto the input's element
+ * shares (the guard's multiplicative correction, twice) moves no species by more than proj_max (relative) and leaves
+ * the guard's drift test passed. Accepted cells take the proposal (steps 0, done 1, flag 0). Rejected cells, and a
+ * seeded draw of one accepted cell in audit_every (0: none), are solved by the solver's Rodas3 path (its precision)
+ * with its guard and recovery, in the same call, with no host synchronisation. The audited cells' proposals go to
+ * audit_x [audit_cap][ns] (their cells to audit_cells, *audit_count of them, at most audit_cap) and their relative
+ * error against Rodas3 per species above 1e-20 (else 0) to audit_err [audit_cap][ns]. stats (device uint64[6]) is
+ * incremented by: accepted, audited, refused for range, for spread, for the projection, unusable inputs. count and
+ * total as mx_call's (the queue slot counts every cell).
+ */
+int mx_sur_call(mx_surrogate* s, mx_solver* solver, const double* x, const double* T, const double* P,
+                const double* dt, const double* h_in, const double* J, int64_t B, double rtol, double atol,
+                int32_t max_steps, double spread_max, double proj_max, int32_t audit_every, uint32_t seed,
+                double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag, int32_t* status,
+                int32_t* count, int64_t* total, uint64_t* stats, int32_t* audit_cells, double* audit_x,
+                float* audit_err, int32_t* audit_count, int32_t audit_cap, void* stream, char* err, size_t errlen);
+
+int mx_sur_destroy(mx_surrogate* s);
+
+/* The surrogate's GEMM alone (a building block, exported for tests): C[M, N] = A[M, K] B[N, K]^T, A and B device BF16
+ * row-major with leading dimensions lda, ldb (K and N multiples of 64). mode 0: out FP32 = C; 1: out FP32 = C + bias;
+ * 2: z = C + bias (FP32 [M][ldz] when z is not null), out BF16 = silu(z); 3: out BF16 = C * silu'(z), z read.
+ * *err_flag (device int32) is set when a wait gave up. Asynchronous on stream. */
+int mx_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int64_t M, int32_t N, int32_t K,
+                 int32_t mode, const float* bias, float* z, int32_t ldz, void* out, int32_t ldo, int32_t* err_flag,
+                 void* stream);
 
 /* Release the solver's device memory. Safe on NULL. */
 int mx_destroy(mx_solver* s);

@@ -142,6 +142,38 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         [_P, _P, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, ctypes.c_double, ctypes.c_double, _P, _P],
     ),
     "mx_probe_fp64": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
+    "mx_set_precision": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_double]),
+    "mx_sur_create": (
+        ctypes.c_int,
+        [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+         ctypes.c_int32, ctypes.POINTER(_P), _ERR, ctypes.c_size_t],
+    ),  # fmt: skip
+    "mx_sur_info": (ctypes.c_int, [_P, _P, ctypes.c_int32]),
+    "mx_sur_set_scaling": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "mx_sur_features": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, ctypes.c_int64, _P, _P, _P]),
+    "mx_sur_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, _P]),
+    "mx_sur_train_step": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int64, ctypes.c_float, _P, _P]),
+    "mx_sur_params": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.c_int64]),
+    "mx_sur_set_params": (ctypes.c_int, [_P, _P, ctypes.c_int64]),
+    "mx_sur_error": (ctypes.c_int, [_P, _P]),
+    "mx_sur_call": (
+        ctypes.c_int,
+        [_P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+         ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32] + [_P] * 13
+        + [ctypes.c_int32, _P, _ERR, ctypes.c_size_t],
+    ),  # fmt: skip
+    "mx_sur_destroy": (ctypes.c_int, [_P]),
+    "mx_gemm_bf16": (
+        ctypes.c_int,
+        [_P, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+         _P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, _P],
+    ),  # fmt: skip
+    "mx_set_escalation_counter": (ctypes.c_int, [_P, _P]),
+    "mx_debug_try_mixed": (
+        ctypes.c_int,
+        [_P, _P, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, ctypes.c_double, ctypes.c_double,
+         ctypes.c_int32, _P, _P],
+    ),  # fmt: skip
     "mx_version": (ctypes.c_char_p, []),
     "mx_warps_per_cell": (ctypes.c_int, []),
 }

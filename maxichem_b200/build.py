@@ -7,10 +7,10 @@ import subprocess
 from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
-SOURCES = [PACKAGE / "csrc" / "maxichem_b200.cu", PACKAGE / "csrc" / "derivatives.cu", PACKAGE / "csrc" / "coupling.cu",
-           PACKAGE / "csrc" / "export.cpp"]
+SOURCES = [PACKAGE / "csrc" / "maxichem_b200.cu", PACKAGE / "csrc" / "mixed.cu", PACKAGE / "csrc" / "surrogate.cu",
+           PACKAGE / "csrc" / "derivatives.cu", PACKAGE / "csrc" / "coupling.cu", PACKAGE / "csrc" / "export.cpp"]
 HEADERS = [PACKAGE / "csrc" / "device.cuh", PACKAGE / "csrc" / "solver.cuh", PACKAGE / "csrc" / "jvp.cuh",
-           PACKAGE / "csrc" / "vjp.cuh", PACKAGE.parent / "include" / "maxichem_b200.h"]
+           PACKAGE / "csrc" / "vjp.cuh", PACKAGE / "csrc" / "gemm.cuh", PACKAGE.parent / "include" / "maxichem_b200.h"]
 OUTPUT = PACKAGE / "_build" / "libmaxichem_b200.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -43,8 +43,11 @@ struct Net {
   const uint16_t* sv_rows[2];
   const uint32_t* jt[2];
   const uint16_t* jd[2];
-  // shared-memory layout
-  int ld, oA, oK, oV, on, oN, oY, oF, oU, oK1, oK2, oK3, oK4, oD, oRed, oInts, oPart, oG, doubles;
+  // shared-memory layout (offsets in doubles); a_doubles: the matrix region's size in doubles. The mixed-precision
+  // layout adds the row scales (oS), the Jacobian's diagonal (oDg), n at the try's state (onN), w (oW), the
+  // residual (oR) and a stage's right side (oB); the plain layout leaves them 0.
+  int ld, oA, oK, oV, on, oN, oY, oF, oU, oK1, oK2, oK3, oK4, oD, oRed, oInts, oPart, oG, doubles, a_doubles;
+  int oS, oDg, onN, oW, oR, oB;
 };
 
 struct CallArgs {
@@ -57,6 +60,10 @@ struct CallArgs {
   double* steps;
   int *flag, *status, *count, *list;
   unsigned long long* tries;  // nullable: [0] tries, [1] tries after a rejection, [2] recovery tries
+  const int* in_list;  // list-mode kernels: the cells to step, in_count[0] of them (in_count[1]: their queue)
+  int* in_count;
+  int* sel;        // the mixed kernel's hand-backs for the plain kernel, sel_count[0] of them
+  int* sel_count;
 };
 
 // Pointers into one CTA's shared memory.
@@ -190,6 +197,35 @@ __device__ __forceinline__ void cell_rates(const Net& net, const Cell& c, double
 // A barrier over the threads of a group: named barrier id (0 is __syncthreads' own) over n threads.
 __device__ __forceinline__ void group_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 
+// S v's pieces into part: each thread of the group its pieces (ascending reactions) from its coalesced word stream;
+// v[nr] = 0 pads. Row i of S v is then part[sv_row_ptr[i]] + ... in order (sv_row of the caller).
+__device__ __forceinline__ void sv_pieces_of(const Net& net, const Cell& c, const double* v, int gtid, int gnt) {
+  const int g = gnt == net.st_threads[0] ? 0 : 1;
+  const uint16_t* __restrict__ sw = net.sv[g] + gtid;
+  const uint16_t* __restrict__ sr = net.sv_rows[g] + gtid;
+  double s = 0.0;
+  int piece = 0;
+  const int rounds = net.sv_rounds[g];
+#pragma unroll 4
+  for (int q = 0; q < rounds; q++) {
+    const unsigned w = __ldg(sw + q * gnt);
+    s = fma(code_coefficient(w >> 11), v[w & 0x7ffu], s);
+    if (w & 0x2000u) {
+      c.part[__ldg(sr + piece * gnt)] = s;
+      s = 0.0;
+      piece++;
+    }
+  }
+}
+
+// Row i of S v from its pieces, added in order.
+__device__ __forceinline__ double sv_row(const Net& net, const Cell& c, int i) {
+  const int p0 = __ldg(net.sv_row_ptr + i), p1 = __ldg(net.sv_row_ptr + i + 1);
+  double r = c.part[p0];
+  for (int p = p0 + 1; p < p1; p++) r += c.part[p];
+  return r;
+}
+
 // F = (ntot / nd) S v(n) at Y, u0 = S v / nd into U when u0; n = nd Y / ntot. Returns ntot. Run by a group of whole
 // warps (gtid its thread index, gnt its size, synchronised by named barrier bar); three barriers.
 __device__ __forceinline__ double rhs(const Net& net, const Cell& c, const double* Y, bool u0, double nd, int gtid, int gnt, int bar) {
@@ -209,29 +245,11 @@ __device__ __forceinline__ double rhs(const Net& net, const Cell& c, const doubl
     c.v[r] = a - b;
   }
   group_sync(bar, gnt);
-  // S v: each thread its pieces (ascending reactions) from its coalesced word stream into part; v[nr] = 0 pads
-  const int g = gnt == net.st_threads[0] ? 0 : 1;
-  const uint16_t* __restrict__ sw = net.sv[g] + gtid;
-  const uint16_t* __restrict__ sr = net.sv_rows[g] + gtid;
-  double s = 0.0;
-  int piece = 0;
-  const int rounds = net.sv_rounds[g];
-#pragma unroll 4
-  for (int q = 0; q < rounds; q++) {
-    const unsigned w = __ldg(sw + q * gnt);
-    s = fma(code_coefficient(w >> 11), c.v[w & 0x7ffu], s);
-    if (w & 0x2000u) {
-      c.part[__ldg(sr + piece * gnt)] = s;
-      s = 0.0;
-      piece++;
-    }
-  }
+  sv_pieces_of(net, c, c.v, gtid, gnt);
   group_sync(bar, gnt);
   // each row: its pieces added in order
   for (int i = gtid; i < ns; i += gnt) {
-    const int p0 = __ldg(net.sv_row_ptr + i), p1 = __ldg(net.sv_row_ptr + i + 1);
-    double r = c.part[p0];
-    for (int p = p0 + 1; p < p1; p++) r += c.part[p];
+    const double r = sv_row(net, c, i);
     c.F[i] = r * ixf;
     if (u0) c.U[i] = r / nd;
   }
@@ -285,9 +303,13 @@ __device__ __forceinline__ void jacobian_w(const Net& net, const Cell& c, double
 // row, warp syncs only) while warps 1-3 apply it to the columns past the next panel, as a rank-PANEL update in 4 x 4
 // register tiles (rows and columns cyclic, so a warp's loads are broadcast or consecutive).
 
+// the element type's correctly rounded reciprocal (FP64 for the plain path, FP32 for the mixed path's factors)
+__device__ __forceinline__ double rcp_rn(double a) { return __drcp_rn(a); }
+__device__ __forceinline__ float rcp_rn(float a) { return __frcp_rn(a); }
+
 // the trailing update of rows ke.. and columns cs.. (cs >= ke) by NT threads
-template <int NT>
-__device__ __forceinline__ void trailing_update_from(double* A, int ld, int kb, int nb, int ke, int cs, int ns, int tid) {
+template <int NT, typename T>
+__device__ __forceinline__ void trailing_update_from(T* A, int ld, int kb, int nb, int ke, int cs, int ns, int tid) {
   constexpr int CG = 16, RG = NT / CG;
   const int cg = tid % CG, rg = tid / CG, m = ns - ke, mc = ns - cs;
   for (int rb = rg; rb < m; rb += 4 * RG) {
@@ -301,7 +323,7 @@ __device__ __forceinline__ void trailing_update_from(double* A, int ld, int kb, 
         cok[a] = cb + CG * a < mc;
         col[a] = cs + (cok[a] ? cb + CG * a : 0);
       }
-      double acc[4][4];
+      T acc[4][4];
 #pragma unroll
       for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -309,7 +331,7 @@ __device__ __forceinline__ void trailing_update_from(double* A, int ld, int kb, 
 #pragma unroll 2
       for (int t = 0; t < PANEL; t++) {
         if (t < nb) {
-          double l[4], u[4];
+          T l[4], u[4];
 #pragma unroll
           for (int a = 0; a < 4; a++) {
             l[a] = A[row[a] * ld + kb + t];
@@ -331,18 +353,19 @@ __device__ __forceinline__ void trailing_update_from(double* A, int ld, int kb, 
 }
 
 // the panel kb .. kb + nb - 1 on one warp (lane), warp-level syncs only
-__device__ __forceinline__ void panel_warp(double* A, int ld, double* dinv, int kb, int nb, int ns, int lane) {
+template <typename T>
+__device__ __forceinline__ void panel_warp(T* A, int ld, T* dinv, int kb, int nb, int ns, int lane) {
   const int ke = kb + nb;
-  if (lane == 0) dinv[kb] = __drcp_rn(A[kb * ld + kb]);
+  if (lane == 0) dinv[kb] = rcp_rn(A[kb * ld + kb]);
   __syncwarp();
   for (int k = kb; k < ke; k++) {
-    const double d = dinv[k];
-    double piv[PANEL];
+    const T d = dinv[k];
+    T piv[PANEL];
 #pragma unroll
-    for (int jj = 1; jj < PANEL; jj++) piv[jj] = k + jj < ke ? A[k * ld + k + jj] : 0.0;
+    for (int jj = 1; jj < PANEL; jj++) piv[jj] = k + jj < ke ? A[k * ld + k + jj] : T(0);
     for (int i = k + 1 + lane; i < ns; i += 32) {
-      double* ai = A + i * ld;
-      const double l = ai[k] * d;
+      T* ai = A + i * ld;
+      const T l = ai[k] * d;
       ai[k] = l;
 #pragma unroll
       for (int jj = 1; jj < PANEL; jj++)
@@ -350,15 +373,15 @@ __device__ __forceinline__ void panel_warp(double* A, int ld, double* dinv, int 
     }
     // the next pivot is final now and its row is lane 0's (its first row), so lane 0 takes the reciprocal of its own
     // write, after the row loop
-    if (lane == 0 && k + 1 < ke) dinv[k + 1] = __drcp_rn(A[(k + 1) * ld + k + 1]);
+    if (lane == 0 && k + 1 < ke) dinv[k + 1] = rcp_rn(A[(k + 1) * ld + k + 1]);
     __syncwarp();
   }
 }
 
 // the blocked LU with a lookahead of one panel: while warps 1-3 apply panel p to the columns past panel p + 1, warp 0
 // applies it to panel p + 1's columns and factors panel p + 1. Each entry takes its updates in ascending pivot order.
-template <int NT>
-__device__ __forceinline__ void lu_factor(const Net& net, double* A, double* dinv, int tid) {
+template <int NT, typename T>
+__device__ __forceinline__ void lu_factor(const Net& net, T* A, T* dinv, int tid) {
   const int ns = net.ns, ld = net.ld, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) panel_warp(A, ld, dinv, 0, min(PANEL, ns), ns, lane);
   __syncthreads();
@@ -366,13 +389,13 @@ __device__ __forceinline__ void lu_factor(const Net& net, double* A, double* din
     const int ke = min(kb + PANEL, ns), nb = ke - kb;
     if (ke == ns) break;
     for (int j = ke + tid; j < ns; j += NT) {  // the block's pivot rows beyond the panel
-      double row[PANEL];
+      T row[PANEL];
 #pragma unroll
-      for (int s = 0; s < PANEL; s++) row[s] = s < nb ? A[(kb + s) * ld + j] : 0.0;
+      for (int s = 0; s < PANEL; s++) row[s] = s < nb ? A[(kb + s) * ld + j] : T(0);
 #pragma unroll
       for (int s = 1; s < PANEL; s++) {
         if (s < nb) {
-          double a = row[s];
+          T a = row[s];
 #pragma unroll
           for (int t = 0; t < PANEL; t++)
             if (t < s) a = fma(-A[(kb + s) * ld + kb + t], row[t], a);
@@ -385,12 +408,12 @@ __device__ __forceinline__ void lu_factor(const Net& net, double* A, double* din
     const int ken = min(ke + PANEL, ns);
     if (warp == 0) {
       for (int i = ke + lane; i < ns; i += 32) {  // panel p + 1's columns, rows ke..
-        double* ai = A + i * ld;
-        double l[PANEL];
+        T* ai = A + i * ld;
+        T l[PANEL];
 #pragma unroll
-        for (int t = 0; t < PANEL; t++) l[t] = t < nb ? ai[kb + t] : 0.0;
+        for (int t = 0; t < PANEL; t++) l[t] = t < nb ? ai[kb + t] : T(0);
         for (int j = ke; j < ken; j++) {
-          double acc = ai[j];
+          T acc = ai[j];
 #pragma unroll
           for (int t = 0; t < PANEL; t++)
             if (t < nb) acc = fma(-l[t], A[(kb + t) * ld + j], acc);
@@ -400,7 +423,7 @@ __device__ __forceinline__ void lu_factor(const Net& net, double* A, double* din
       __syncwarp();
       panel_warp(A, ld, dinv, ke, ken - ke, ns, lane);
     } else {
-      trailing_update_from<NT - 32>(A, ld, kb, nb, ke, ken, ns, tid - 32);
+      trailing_update_from<NT - 32, T>(A, ld, kb, nb, ke, ken, ns, tid - 32);
     }
     __syncthreads();
   }
@@ -422,37 +445,30 @@ __device__ __forceinline__ double pick(const double (&a)[R], int idx) {
 // column of L or U is loaded while the current pivot is applied. A lane whose row takes no update from pivot k uses
 // the multiplier 0, and fma(-0, y, a) = a for finite y. Each entry receives the one-pivot sweep's fma's in its order.
 // Not inlined: the call kernel solves at four places, and one copy of the code keeps the instruction cache warm.
-template <int R, int NV>
-__device__ __noinline__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1,
-                                         int lane) {
+// The forward and backward sweeps of M0^-1 on NV register-held vectors (a: lane l holds rows l + 32 p; d: 1 / U_kk),
+// the body of lu_solve (double) and of the mixed path's solve (float). On return a[v][p] * d[p] is the solution.
+template <int R, int NV, typename T>
+__device__ __forceinline__ void lu_sweep(const Net& net, const T* A, T (&a)[NV][R], const T (&d)[R], int lane) {
   const int ns = net.ns, ld = net.ld, last = ns - 1;
-  double a[NV][R], d[R];
-#pragma unroll
-  for (int p = 0; p < R; p++) {
-    const int i = lane + 32 * p;
-    d[p] = i < ns ? dinv[i] : 0.0;
-    a[0][p] = i < ns ? y0[i] : 0.0;
-    if (NV == 2) a[NV - 1][p] = i < ns ? y1[i] : 0.0;
-  }
 #pragma unroll
   for (int c = 0; c < R; c++) {  // forward: pivots 32c .. 32c + 31
     const int k0 = 32 * c, k1 = min(k0 + 32, last);
     if (k0 >= k1) break;
-    double m[R];
+    T m[R];
 #pragma unroll
     for (int p = c; p < R; p++) m[p] = A[min(lane + 32 * p, last) * ld + k0];
 #pragma unroll 2
     for (int k = k0; k < k1; k++) {
-      double yk[NV];
+      T yk[NV];
 #pragma unroll
       for (int v = 0; v < NV; v++) yk[v] = __shfl_sync(FULL, a[v][c], k & 31);
-      double mn[R];
+      T mn[R];
 #pragma unroll
       for (int p = c; p < R; p++) mn[p] = A[min(lane + 32 * p, last) * ld + min(k + 1, last)];
 #pragma unroll
       for (int p = c; p < R; p++) {
         const bool act = (p > c ? true : lane > k - k0) && lane + 32 * p < ns;
-        const double mm = act ? m[p] : 0.0;
+        const T mm = act ? m[p] : T(0);
 #pragma unroll
         for (int v = 0; v < NV; v++) a[v][p] = fma(-mm, yk[v], a[v][p]);
         m[p] = mn[p];
@@ -463,27 +479,48 @@ __device__ __noinline__ void lu_solve(const Net& net, const double* A, const dou
   for (int c = R - 1; c >= 0; c--) {  // backward: pivots 32c + 31 .. 32c (down to 1)
     const int k0 = 32 * c, khi = min(k0 + 31, last), klo = max(k0, 1);
     if (khi < klo) continue;
-    double m[R];
+    T m[R];
 #pragma unroll
     for (int p = 0; p <= c; p++) m[p] = A[min(lane + 32 * p, last) * ld + khi];
 #pragma unroll 2
     for (int k = khi; k >= klo; k--) {
-      double z[NV];
+      T z[NV];
 #pragma unroll
       for (int v = 0; v < NV; v++) z[v] = __shfl_sync(FULL, a[v][c] * d[c], k & 31);
-      double mn[R];
+      T mn[R];
 #pragma unroll
       for (int p = 0; p <= c; p++) mn[p] = A[min(lane + 32 * p, last) * ld + max(k - 1, 0)];
 #pragma unroll
       for (int p = 0; p <= c; p++) {
         const bool act = p < c ? true : lane < k - k0;
-        const double mm = act ? m[p] : 0.0;
+        const T mm = act ? m[p] : T(0);
 #pragma unroll
         for (int v = 0; v < NV; v++) a[v][p] = fma(-mm, z[v], a[v][p]);
         m[p] = mn[p];
       }
     }
   }
+}
+
+// y <- M0^-1 y on one warp for NV vectors (1 or 2) with the factors of lu_factor: lane l holds rows l + 32 p.
+// Forward unit L in ascending k, U in descending k with x_k = a_k / U_kk (msolve, common.cuh:504-522). Pivots are
+// taken 32 at a time, so the pivot's value comes from a register chosen at compile time (c) and one shuffle; the next
+// column of L or U is loaded while the current pivot is applied. A lane whose row takes no update from pivot k uses
+// the multiplier 0, and fma(-0, y, a) = a for finite y. Each entry receives the one-pivot sweep's fma's in its order.
+// Not inlined: the call kernel solves at four places, and one copy of the code keeps the instruction cache warm.
+template <int R, int NV>
+__device__ __noinline__ void lu_solve(const Net& net, const double* A, const double* dinv, double* y0, double* y1,
+                                         int lane) {
+  const int ns = net.ns;
+  double a[NV][R], d[R];
+#pragma unroll
+  for (int p = 0; p < R; p++) {
+    const int i = lane + 32 * p;
+    d[p] = i < ns ? dinv[i] : 0.0;
+    a[0][p] = i < ns ? y0[i] : 0.0;
+    if (NV == 2) a[NV - 1][p] = i < ns ? y1[i] : 0.0;
+  }
+  lu_sweep<R, NV, double>(net, A, a, d, lane);
   __syncwarp();
 #pragma unroll
   for (int p = 0; p < R; p++) {
@@ -746,7 +783,7 @@ static __device__ __noinline__ int check_cell(const Net& net, const double* x0, 
 __device__ __forceinline__ void stage_guard_inputs(const Net& net, const Cell& c, const double* x0, int tid, int nt,
                                                    const double** at, const double** xin) {
   const int ns = net.ns, na = ns * net.nel;
-  if (na + ns > ns * net.ld) return;
+  if (na + ns > net.a_doubles) return;
   for (int e = tid; e < na; e += nt) c.A[e] = __ldg(net.atoms + e);
   for (int i = tid; i < ns; i += nt) c.A[na + i] = x0[i];
   *at = c.A;

@@ -24,8 +24,9 @@ namespace {
 enum { PH_RATES, PH_RHS_JAC, PH_LU, PH_STAGE12, PH_STAGE3, PH_STAGE4, PH_CONTROL, PH_OUTPUT, PH_COUNT };
 
 // The call kernel: screening, rates, Rodas3 steps, output and the guard, per cell (call.cuh:5-177, guard.cuh:114-140).
-// PROF: also sum clock64 cycles per phase into prof[PH_COUNT].
-template <int W, int R, bool PROF>
+// PROF: also sum clock64 cycles per phase into prof[PH_COUNT]. LIST: step only the cells a.in_list lists
+// (a.in_count[0] of them: the mixed kernel's hand-backs, or the surrogate's fallbacks), with a.in_count[1] as the queue.
+template <int W, int R, bool PROF, bool LIST = false>
 __global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const CallArgs a, long long* prof) {
   extern __shared__ double smem[];
   const Cell c = cell_arrays(net, smem);
@@ -43,8 +44,10 @@ __global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const Ca
       t0 = t;
     }
   };
-  int cell = (int)blockIdx.x;
-  while (cell < a.B) {
+  const int nb = LIST ? a.in_count[0] : a.B;
+  int q = (int)blockIdx.x;
+  while (q < nb) {
+    const int cell = LIST ? a.in_list[q] : q;
     const double Tc = a.T[cell], dt = a.dt[cell], hin = a.h_in[cell];
     const double nd = a.P[cell] / (MX_KB * Tc);
     const double* x0 = a.x + (size_t)cell * ns;
@@ -196,19 +199,19 @@ __global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const Ca
           atomicAdd(a.tries, (unsigned long long)tries);
           atomicAdd(a.tries + 1, (unsigned long long)retries);
         }
-        c.ints[1] = (int)(gridDim.x + atomicAdd(a.count + MX_COUNT_QUEUE, 1));
+        c.ints[1] = (int)(gridDim.x + atomicAdd(LIST ? a.in_count + 1 : a.count + MX_COUNT_QUEUE, 1));
       }
     }
     __syncthreads();
     double* xo = a.x_out + (size_t)cell * ns;
     for (int i = tid; i < ns; i += nt) xo[i] = c.Y[i];
-    cell = c.ints[1];
+    q = c.ints[1];
     __syncthreads();
     mark(PH_OUTPUT);
   }
   if (PROF && tid == 0) {
 #pragma unroll
-    for (int q = 0; q < PH_COUNT; q++) atomicAdd((unsigned long long*)prof + q, (unsigned long long)ph[q]);
+    for (int p = 0; p < PH_COUNT; p++) atomicAdd((unsigned long long*)prof + p, (unsigned long long)ph[p]);
   }
 }
 
@@ -513,22 +516,24 @@ __global__ void __launch_bounds__(128) guard_kernel(const Net net, const double*
 }
 
 template <int R>
-void kernels_for(CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg, TimeFn* tim) {
-  *tim = time_phases_kernel<WARPS, R>;
-  *call = call_kernel<WARPS, R, false>;
-  *prof = call_kernel<WARPS, R, true>;
-  *rec = recover_kernel<WARPS, R>;
-  *dbg = debug_try_kernel<WARPS, R>;
+void kernels_for(mx_solver* s) {
+  s->timer = time_phases_kernel<WARPS, R>;
+  s->call = call_kernel<WARPS, R, false>;
+  s->call_prof = call_kernel<WARPS, R, true>;
+  s->call_list = call_kernel<WARPS, R, false, true>;
+  s->recover = recover_kernel<WARPS, R>;
+  s->debug = debug_try_kernel<WARPS, R>;
+  s->rows_per_lane = R;
 }
 
 // rows per lane of the warp solves: species up to 32, 64, 96, 128, 256
-bool pick_kernels(int ns, CallFn* call, CallFn* prof, RecoverFn* rec, DebugFn* dbg, TimeFn* tim, int* r) {
+bool pick_kernels(int ns, mx_solver* s) {
   const int need = (ns + 31) / 32;
-  if (need <= 1) { kernels_for<1>(call, prof, rec, dbg, tim); *r = 1; return true; }
-  if (need <= 2) { kernels_for<2>(call, prof, rec, dbg, tim); *r = 2; return true; }
-  if (need <= 3) { kernels_for<3>(call, prof, rec, dbg, tim); *r = 3; return true; }
-  if (need <= 4) { kernels_for<4>(call, prof, rec, dbg, tim); *r = 4; return true; }
-  if (need <= 8) { kernels_for<8>(call, prof, rec, dbg, tim); *r = 8; return true; }
+  if (need <= 1) { kernels_for<1>(s); return true; }
+  if (need <= 2) { kernels_for<2>(s); return true; }
+  if (need <= 3) { kernels_for<3>(s); return true; }
+  if (need <= 4) { kernels_for<4>(s); return true; }
+  if (need <= 8) { kernels_for<8>(s); return true; }
   return false;
 }
 
@@ -541,7 +546,33 @@ void release(mx_solver* s) {
   s->buffers.clear();
   if (s->list) cudaFree(s->list);
   s->list = nullptr;
+  if (s->sel) cudaFree(s->sel);
+  s->sel = nullptr;
+  if (s->sel_count) cudaFree(s->sel_count);
+  s->sel_count = nullptr;
   mx_release_derivatives(s);
+}
+
+// The mixed path's list of cells for the plain kernel, grown to B cells, and its two counters.
+int grow_sel(mx_solver* s, int64_t B, char* err, size_t errlen) {
+  cudaError_t e = cudaSuccess;
+  if (!s->sel_count) e = cudaMalloc(&s->sel_count, 2 * sizeof(int));
+  if (e == cudaSuccess && B > s->sel_capacity) {
+    if (s->sel) cudaFree(s->sel);
+    s->sel = nullptr;
+    s->sel_capacity = 0;
+    e = cudaMalloc(&s->sel, (size_t)B * sizeof(int));
+    if (e == cudaSuccess) s->sel_capacity = B;
+  }
+  if (e != cudaSuccess) {
+    set_error(err, errlen, "mx_call: the mixed path's list of %lld cells: %s", (long long)B, cudaGetErrorString(e));
+    return MX_ERR_CUDA;
+  }
+  return MX_OK;
+}
+
+__global__ void add_escalated_kernel(const int* sel_count, long long* escalated) {
+  if (threadIdx.x == 0) escalated[0] += sel_count[0];
 }
 
 }  // namespace
@@ -581,7 +612,7 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   double etot = 0.0;
   for (int i = 0; i < ns * n->nel; i++) etot += n->atoms[i];
   net.etot = etot;
-  if (!pick_kernels(ns, &s->call, &s->call_prof, &s->recover, &s->debug, &s->timer, &s->rows_per_lane)) {
+  if (!pick_kernels(ns, s)) {
     delete s;
     return MX_ERR_NETWORK;
   }
@@ -594,6 +625,7 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
     return o;
   };
   net.oA = take(ns * net.ld);
+  net.a_doubles = ns * net.ld;
   net.oK = take(2 * nr + 2);
   net.oV = take(std::max(nr + 1, ns + 1));
   net.on = take(ns + 1);
@@ -636,6 +668,8 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
     e = cudaFuncSetAttribute((const void*)s->timer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)s->call_prof, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)s->call_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->call_ctas, (const void*)s->call, 32 * WARPS, s->smem);
   if (e == cudaSuccess)
@@ -705,16 +739,14 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
     delete s;
     return MX_ERR_CUDA;
   }
+  const int mrc = mx_mixed_prepare(s, n->n_pieces, err, errlen);
+  if (mrc) {
+    release(s);
+    delete s;
+    return mrc;
+  }
   *out = s;
   return MX_OK;
-}
-
-// The call kernel's grid: persistent over the cell queue with grid_ctas CTAs per SM (the occupancy limit by
-// default), or one CTA per cell (grid_ctas 0: every CTA takes one cell and finds the queue past the batch).
-static int call_grid(const mx_solver* s, int64_t B) {
-  if (s->grid_ctas == 0) return (int)B;
-  const int per_sm = s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas;
-  return (int)std::min<int64_t>(B, (int64_t)per_sm * s->sms);
 }
 
 extern "C" int mx_call(mx_solver* s, const double* x, const double* T, const double* P, const double* dt,
@@ -750,27 +782,59 @@ extern "C" int mx_call(mx_solver* s, const double* x, const double* T, const dou
   cudaStream_t st = (cudaStream_t)stream;
   int rc = grow_list(s, std::max<int64_t>(B, 1), err, errlen);
   if (rc) return rc;
+  const bool mixed = s->precision == MX_PRECISION_MIXED && B > 0;
+  if (mixed) {
+    rc = grow_sel(s, B, err, errlen);
+    if (rc) return rc;
+  }
   cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
+  if (e == cudaSuccess && mixed) e = cudaMemsetAsync(s->sel_count, 0, 2 * sizeof(int), st);
   if (e == cudaSuccess && B > 0) {
     CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status, count,
-               s->list, s->tries};
+               s->list, s->tries, nullptr, nullptr, s->sel, s->sel_count};
     const int grid = call_grid(s, B);
-    if (s->phases)
+    if (mixed) {
+      // the mixed kernel, then the plain kernel on the cells it handed back (it returns at once when none)
+      e = mx_mixed_launch(s, a, B, false, st);
+      CallArgs back = a;
+      back.in_list = s->sel;
+      back.in_count = s->sel_count;
+      if (e == cudaSuccess) s->call_list<<<grid, 32 * WARPS, s->smem, st>>>(s->net, back, nullptr);
+    } else if (s->phases) {
       s->call_prof<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, s->phases);
-    else
+    } else {
       s->call<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, nullptr);
+    }
     const int rgrid = (int)std::min<int64_t>(B, (int64_t)s->recover_ctas * s->sms);
-    s->recover<<<rgrid, 32 * WARPS, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
-    e = cudaGetLastError();
+    if (e == cudaSuccess) s->recover<<<rgrid, 32 * WARPS, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
+    if (e == cudaSuccess) e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
     add_counts_kernel<<<1, 32, 0, st>>>(count, (long long*)total);
+    if (mixed && s->escalated) add_escalated_kernel<<<1, 32, 0, st>>>(s->sel_count, s->escalated);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) {
     set_error(err, errlen, "mx_call: %s", cudaGetErrorString(e));
     return MX_ERR_CUDA;
   }
+  return MX_OK;
+}
+
+extern "C" int mx_set_precision(mx_solver* s, int32_t precision, int32_t sweeps, double tol) {
+  if (!s) return MX_ERR_CLOSED;
+  if ((precision != MX_PRECISION_FP64 && precision != MX_PRECISION_MIXED) || sweeps < 1 ||
+      sweeps > MX_MIXED_MAX_SWEEPS || !(tol > 0.0 && tol < 1e300))
+    return MX_ERR_ARGUMENT;
+  s->precision = precision;
+  s->sweeps = sweeps;
+  s->mixed_tol = tol;
+  return MX_OK;
+}
+
+extern "C" int mx_set_escalation_counter(mx_solver* s, int64_t* counter) {
+  if (!s) return MX_ERR_CLOSED;
+  s->escalated = (long long*)counter;
   return MX_OK;
 }
 
@@ -806,14 +870,15 @@ extern "C" int mx_guard(mx_solver* s, const double* x, double* x_out, const int3
 extern "C" int mx_info(const mx_solver* s, int32_t* values, int32_t n) {
   if (!s || !values) return MX_ERR_ARGUMENT;
   const int32_t v[] = {WARPS, s->rows_per_lane, (int32_t)s->smem, s->call_ctas, s->recover_ctas, s->sms, s->net.ld,
-                       s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas, (int32_t)s->list_capacity};
+                       s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas, (int32_t)s->list_capacity,
+                       (int32_t)s->mixed_smem, s->mixed_ctas, s->precision, s->sweeps};
   for (int i = 0; i < n && i < (int)(sizeof v / sizeof v[0]); i++) values[i] = v[i];
   return MX_OK;
 }
 
 extern "C" int mx_set_grid(mx_solver* s, int32_t ctas_per_sm) {
   if (!s) return MX_ERR_CLOSED;
-  if (ctas_per_sm < -1 || ctas_per_sm > s->call_ctas) return MX_ERR_ARGUMENT;
+  if (ctas_per_sm < -1 || ctas_per_sm > std::max(s->call_ctas, s->mixed_ctas)) return MX_ERR_ARGUMENT;
   s->grid_ctas = ctas_per_sm;
   return MX_OK;
 }

@@ -16,6 +16,9 @@ typedef void (*CallFn)(const mx::Net, const mx::CallArgs, long long*);
 typedef void (*DebugFn)(const mx::Net, const double*, double, double, double, const double*, double, double, double*);
 typedef void (*RecoverFn)(const mx::Net, const mx::CallArgs, int);
 typedef void (*TimeFn)(const mx::Net, const double*, double, double, double, const double*, int, long long*);
+typedef void (*MixedFn)(const mx::Net, const mx::CallArgs, int, double, long long*);
+typedef void (*MixedDebugFn)(const mx::Net, const double*, double, double, double, const double*, double, double, int,
+                             double*);
 
 struct mx_derivatives;  // the tangent and adjoint kernels' state (derivatives.cu)
 
@@ -25,6 +28,7 @@ struct mx_solver {
   std::vector<void*> buffers;
   CallFn call = nullptr;
   CallFn call_prof = nullptr;
+  CallFn call_list = nullptr;  // the plain kernel over the cells the mixed kernel listed (a.sel)
   RecoverFn recover = nullptr;
   DebugFn debug = nullptr;
   TimeFn timer = nullptr;
@@ -39,7 +43,30 @@ struct mx_solver {
   std::vector<uint64_t> rx8_host;  // the reactions' slots, for the adjoint's species gather table
   std::vector<uint64_t> st8_host;  // S's columns: per reaction up to 6 (species byte, coefficient code) pairs
   mx_derivatives* deriv = nullptr;  // the tangent and adjoint kernels' state, at their first call
+  // the mixed-precision path (mixed.cu): its layout, kernels and settings, and the list of cells it hands back
+  mx::Net net32{};
+  MixedFn mixed = nullptr, mixed_prof = nullptr, mixed_list = nullptr;
+  MixedDebugFn mixed_debug = nullptr;
+  size_t mixed_smem = 0;
+  int mixed_ctas = 0;
+  int precision = MX_PRECISION_FP64, sweeps = 1;
+  double mixed_tol = MX_MIXED_TOL;
+  int* sel = nullptr;        // cells the mixed kernel listed for the plain kernel [B]
+  int64_t sel_capacity = 0;
+  int* sel_count = nullptr;  // device int[2]: listed cells, the plain kernel's queue over them
+  long long* escalated = nullptr;  // a caller's device int64 that later mixed calls add their listed cells to
 };
+
+// The mixed-precision path (mixed.cu): its layout and kernels at mx_create; its launch within mx_call.
+int mx_mixed_prepare(mx_solver* s, int n_pieces, char* err, size_t errlen);
+cudaError_t mx_mixed_launch(mx_solver* s, const mx::CallArgs& a, int64_t B, bool list, cudaStream_t st);
+
+// The call's grid of the plain kernel: persistent CTAs per SM as set by mx_set_grid, or one per cell.
+inline int call_grid(const mx_solver* s, int64_t B) {
+  if (s->grid_ctas == 0) return (int)B;
+  const int per_sm = s->grid_ctas < 0 ? s->call_ctas : std::min(s->grid_ctas, s->call_ctas);
+  return (int)std::min<int64_t>(B, (int64_t)per_sm * s->sms);
+}
 
 // Frees a solver's derivative state and scratch (derivatives.cu); nothing when it has none.
 void mx_release_derivatives(mx_solver* s);

@@ -26,7 +26,10 @@ __all__ = ["ATOL", "COUNTS", "DRIFT", "REC_STEPS", "T_MAX", "T_MIN", "X_SUM_TOL"
 
 _ERRLEN = 1024
 INFO_FIELDS = ("warps", "rows_per_lane", "smem", "call_ctas_per_sm", "recover_ctas_per_sm", "sms", "ld",
-               "grid_ctas_per_sm", "list_cells")
+               "grid_ctas_per_sm", "list_cells", "mixed_smem", "mixed_ctas_per_sm", "precision", "sweeps")
+PRECISIONS = {"fp64": 0, "mixed": 1}
+MIXED_TOL = 1.0  # MX_MIXED_TOL of include/maxichem_b200.h
+MAX_SWEEPS = 4  # MX_MIXED_MAX_SWEEPS
 
 
 class CallResult(NamedTuple):
@@ -120,11 +123,22 @@ class CudaSolver:
     ``drift`` (the guard's element-drift allowance, DRIFT if None) and ``photo`` (the network's photolysis branches
     enter the call, which then takes J). Calls run one at a time on torch's current stream: the scratch, the queues
     and the counts are shared.
+
+    Beyond the reference: ``precision`` "fp64" (the reference's arithmetic) or "mixed" (each try's linear algebra in
+    row-scaled FP32, every stage solve refined ``sweeps`` times against an FP64 residual; a try whose last correction
+    exceeds ``tol`` times the error-control scale has its cell redone in FP64 in the same call, counted in
+    ``escalated``). Results, counts, flags and refusals have the same meaning in both.
     """
 
     def __init__(self, net: VulcanNetwork, device: torch.device | str, *, drift: float | None = None,
-                 photo: bool = False) -> None:
+                 photo: bool = False, precision: str = "fp64", sweeps: int = 1, tol: float = MIXED_TOL) -> None:
         self._handle: ctypes.c_void_p | None = None
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision: one of {sorted(PRECISIONS)} expected, got {precision!r}")
+        if not (isinstance(sweeps, int) and 1 <= sweeps <= MAX_SWEEPS):
+            raise ValueError(f"sweeps: an integer from 1 to {MAX_SWEEPS} expected, got {sweeps!r}")
+        if not (math.isfinite(tol) and tol > 0.0):
+            raise ValueError(f"tol: a finite value above 0 expected, got {tol}")
         if photo and (not net.photo or net.photo_missing):
             raise ValueError(
                 "photo=True needs a network with photolysis branches whose species are all in its species "
@@ -149,9 +163,12 @@ class CudaSolver:
         if rc:
             raise (ValueError if rc in (1, 3) else RuntimeError)(err.value.decode())
         self._handle = handle
-        values = (ctypes.c_int32 * len(INFO_FIELDS))()
-        self._lib.mx_info(self._handle, values, len(INFO_FIELDS))
-        self.info: dict[str, Any] = dict(zip(INFO_FIELDS, list(values)))
+        self.precision, self.sweeps, self.tol = precision, int(sweeps), float(tol)
+        if self._lib.mx_set_precision(self._handle, PRECISIONS[precision], self.sweeps, self.tol):
+            raise ValueError(f"precision {precision!r}, sweeps {sweeps}, tol {tol}: refused by the library")
+        self.escalated = torch.zeros(1, dtype=torch.int64, device=self.dev)
+        self._lib.mx_set_escalation_counter(self._handle, self.escalated.data_ptr())
+        self.info: dict[str, Any] = self.layout()
         self.info.update(ns=self.ns, nr=self.nr, nj=self.nj, drift=self.drift, flops=dict(self.tab.flops))
 
     # lifetime (_solver.py:142-167)

@@ -1,0 +1,68 @@
+"""The surrogate's tcgen05 BF16 GEMM (mx_gemm_bf16) against a plain PyTorch FP32 computation on the same BF16
+operands: every epilogue, full and partial row tiles, both column tile widths, several K."""
+
+import numpy as np
+import pytest
+import torch
+
+from maxichem_b200 import abi
+
+pytestmark = pytest.mark.gpu
+STORE, BIAS, BIAS_SILU, DSILU = 0, 1, 2, 3
+
+
+def run(mode, A, B, bias=None, z=None):
+    M, K = A.shape
+    N = B.shape[0]
+    dev = A.device
+    flag = torch.zeros(1, dtype=torch.int32, device=dev)
+    if mode in (STORE, BIAS):
+        out = torch.full((M, N), float("nan"), dtype=torch.float32, device=dev)
+    else:
+        out = torch.full((M, N), float("nan"), dtype=torch.bfloat16, device=dev)
+    zt = z if z is not None else (torch.full((M, N), float("nan"), dtype=torch.float32, device=dev)
+                                  if mode == BIAS_SILU else None)  # fmt: skip
+    p = lambda t: None if t is None else t.data_ptr()
+    rc = abi.library().mx_gemm_bf16(p(A), K, p(B), K, M, N, K, mode, p(bias), p(zt), N, p(out), N, p(flag),
+                                    torch.cuda.current_stream(dev).cuda_stream)  # fmt: skip
+    assert rc == 0
+    torch.cuda.synchronize(dev)
+    assert int(flag.item()) == 0
+    return out, zt
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 128, 512), (1000, 320, 512), (4096, 512, 128), (77, 64, 192)])
+def test_every_epilogue_matches_an_fp32_product(gpu, M, N, K):
+    g = torch.Generator(device=gpu)
+    g.manual_seed(M + N + K)
+    A = torch.randn(M, K, device=gpu, generator=g).to(torch.bfloat16)
+    B = (torch.randn(N, K, device=gpu, generator=g) / K**0.5).to(torch.bfloat16)
+    bias = torch.randn(N, device=gpu, generator=g)
+    ref = A.float() @ B.float().T
+    tol = 2e-5 * float(ref.abs().max())
+    out, _ = run(STORE, A, B)
+    assert float((out - ref).abs().max()) <= tol
+    out, _ = run(BIAS, A, B, bias=bias)
+    assert float((out - (ref + bias)).abs().max()) <= tol
+    out, z = run(BIAS_SILU, A, B, bias=bias)
+    zr = ref + bias
+    assert float((z - zr).abs().max()) <= tol
+    silu = zr * torch.sigmoid(zr)
+    # one BF16 rounding of the output: half an ulp of 8 bits of mantissa, plus the product's FP32 difference
+    assert bool(((out.float() - silu).abs() <= silu.abs() * 2**-8 + 2 * tol).all())
+    zin = torch.randn(M, N, device=gpu, generator=g)
+    out, _ = run(DSILU, A, B, z=zin)
+    s = torch.sigmoid(zin)
+    want = ref * s * (1 + zin * (1 - s))
+    assert bool(((out.float() - want).abs() <= want.abs() * 2**-8 + 4 * tol).all())
+
+
+def test_shapes_the_kernel_does_not_take_are_refused(gpu):
+    A = torch.zeros(128, 100, dtype=torch.bfloat16, device=gpu)
+    B = torch.zeros(64, 100, dtype=torch.bfloat16, device=gpu)
+    out = torch.zeros(128, 64, dtype=torch.float32, device=gpu)
+    flag = torch.zeros(1, dtype=torch.int32, device=gpu)
+    rc = abi.library().mx_gemm_bf16(A.data_ptr(), 100, B.data_ptr(), 100, 128, 64, 100, STORE, None, None, 0,
+                                    out.data_ptr(), 64, flag.data_ptr(), None)  # fmt: skip
+    assert rc == 1  # K must be a multiple of 64
+    assert np.isfinite(out.cpu().numpy()).all()

@@ -1,0 +1,134 @@
+"""The learned part on the GPU: features, the network's forward pass and gradients against the CPU reference
+(oracle/surrogate_ref.py, rounding to BF16 where the kernels do), training, and the gated call (no acceptance gives
+the plain call bit for bit; accepted cells conserve their element shares; audited cells carry Rodas3's result and the
+audit measures the proposals' error)."""
+
+import numpy as np
+import pytest
+import torch
+
+import parity
+from maxichem_b200 import surrogate as sg
+from maxichem_b200 import synthetic
+from maxichem_b200.solver import CudaSolver
+from oracle import surrogate_ref as ref
+
+pytestmark = pytest.mark.gpu
+GRAD_RTOL = 5e-3  # per layer, norm-relative: the sums' FP32 order and the odd BF16 rounding flip of dZ
+
+
+def t(a, dev):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+
+
+@pytest.fixture(scope="module")
+def small(gpu, networks):
+    """The 41-species network, its plain solver, and pairs of two chained 300 s calls on 4,096 column cells."""
+    net = networks("cho41")
+    solver = CudaSolver(net, gpu, photo=True)
+    data = sg.pairs(solver, 4096, 2, seed=31)
+    yield net, solver, data
+    solver.close()
+
+
+def test_features_are_the_standardised_logs(small, gpu):
+    net, solver, data = small
+    sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, hidden=128, layers=2, heads=2)
+    raw = sg.raw_features(data.x, data.T, data.P, data.dt, data.J)
+    sur.set_scaling(raw, sg.targets(data.x, data.x_out, data.h_out))
+    feat, inr = sur.features(data.x, data.T, data.P, data.dt, data.J)
+    sc = sur.scaling
+    want = (raw.cpu().numpy() - sc["fmean"]) / np.where(sc["fstd"] > 0, sc["fstd"], 1.0)
+    got = feat.float().cpu().numpy()
+    assert np.abs(got[:, : sur.nf] - ref.bf16(want)).max() <= 2**-7 * np.abs(want).max()
+    assert (got[:, sur.nf :] == 0).all() and bool(inr.bool().all())
+    shifted = data.T.clone()
+    shifted[:5] = 10.0 ** (sc["fhi"][solver.ns] + 0.01)  # T above the training range
+    _, inr2 = sur.features(data.x, shifted, data.P, data.dt, data.J)
+    assert not bool(inr2[:5].bool().any()) and bool(inr2[5:].bool().all())
+    sur.close()
+
+
+def test_gradients_match_the_cpu_reference_layer_by_layer(small, gpu):
+    net, solver, data = small
+    sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, seed=3)  # 4 x 512, 4 heads
+    raw = sg.raw_features(data.x, data.T, data.P, data.dt, data.J)
+    tg = sg.targets(data.x, data.x_out, data.h_out)
+    sur.set_scaling(raw, tg)
+    M = 256
+    feat, _ = sur.features(data.x[:M], data.T[:M], data.P[:M], data.dt[:M], data.J[:M])
+    y = sur.standardised_targets(tg[:M])
+    wts = torch.poisson(torch.ones(M, sur.heads, device=gpu)).float()
+    p0 = sur.params()
+    loss = torch.zeros(1, dtype=torch.float32, device=gpu)
+    sur.train_step(feat, y, wts, 0.0, loss)  # lr 0: the gradients alone
+    sur.check()
+    gpu_grads = sur.unpack(sur.params(1))
+    assert np.array_equal(sur.params(), p0)
+    layers = ref.unpack(p0, sur.shapes)
+    pred, a, z = ref.forward(feat.float().cpu().numpy(), layers)
+    dpred, lossr = ref.loss_grad(pred, y.cpu().numpy(), wts.cpu().numpy(), sur.heads, sur.nt)
+    grads = ref.backward(dpred, layers, a, z)
+    assert abs(float(loss.item()) - lossr) <= 1e-3 * lossr
+    for l, ((gw, gb), (rw, rb)) in enumerate(zip(gpu_grads, grads)):
+        ew = np.linalg.norm(gw - rw) / np.linalg.norm(rw)
+        eb = np.linalg.norm(gb - rb) / max(np.linalg.norm(rb), 1e-30)
+        assert ew <= GRAD_RTOL and eb <= GRAD_RTOL, (l, ew, eb)
+    # the forward pass of the library equals the reference's (same BF16 operands, FP32 sums in another order)
+    got = sur.forward(feat).cpu().numpy()
+    assert np.abs(got - pred).max() <= 1e-3 * np.abs(pred).max()
+    sur.close()
+
+
+def test_training_lowers_the_loss(small, gpu):
+    net, solver, data = small
+    sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, seed=5)
+    hist = sur.fit(data, epochs=6, batch=1024, lr=2e-3)["loss"]
+    assert hist[-1] < 0.5 * hist[0], hist
+    sur.close()
+
+
+def test_a_gate_that_accepts_nothing_gives_the_plain_call(small, gpu):
+    net, solver, data = small
+    sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, seed=7)
+    sur.fit(data, epochs=1, batch=1024)
+    w = synthetic.workload(net, "column", 2048, seed=41)
+    args = [t(a, gpu) for a in (w.x, w.T, w.P, w.dt, w.h)]
+    J = t(w.J, gpu)
+    plain = solver.launch(*args, J=J)
+    counts = solver.fallback
+    gated = sg.GatedSolver(solver, sur, spread_max=0.0, proj_max=0.0, audit_every=0)
+    r = gated(*args, J=J)
+    assert torch.equal(r.x, plain.x) and torch.equal(r.h, plain.h) and torch.equal(r.steps, plain.steps)
+    assert torch.equal(r.done, plain.done) and torch.equal(solver.flag, plain.flag)
+    assert solver.fallback == counts
+    assert gated.counts()["accepted"] == 0
+    sur.close()
+
+
+def test_accepted_cells_conserve_and_audited_cells_are_solved(small, gpu):
+    net, solver, data = small
+    sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, seed=9)
+    sur.fit(data, epochs=4, batch=1024)
+    x, T, P, dt, h, J = data.x_out[:2048], data.T[:2048], data.P[:2048], data.dt[:2048], data.h_out[:2048], data.J[:2048]
+    x = x / x.sum(1, keepdim=True)
+    plain = solver.launch(x, T, P, dt, h, J=J)
+    gated = sg.GatedSolver(solver, sur, spread_max=10.0, proj_max=1.0, audit_every=4, seed=3)  # a loose gate
+    r = gated(x, T, P, dt, h, J=J)
+    c = gated.counts()
+    assert c["accepted"] > 0 and c["audited"] > 0
+    acc = (r.steps == 0) & r.done
+    # accepted: element shares of the input kept (the projection), sum 1
+    sh = lambda q: parity.shares(q.cpu().numpy(), solver.tab.atoms)  # noqa: E731
+    assert np.abs(sh(r.x[acc]) - sh(x[acc])).max() <= 1e-9
+    assert torch.allclose(r.x[acc].sum(1), torch.ones_like(r.x[acc].sum(1)), rtol=0, atol=1e-12)
+    # audited and rejected cells: Rodas3's result bit for bit
+    solved = ~acc
+    assert torch.equal(r.x[solved], plain.x[solved]) and torch.equal(r.steps[solved], plain.steps[solved])
+    n = int(gated.audit_count.item())
+    cells = gated.audit_cells[:n].long()
+    assert bool((r.steps[cells] == plain.steps[cells]).all())
+    prop, truth = gated.audit_x[:n], plain.x[cells]
+    want = torch.where(truth > sg.AUDIT_FLOOR, (prop - truth).abs() / truth, torch.zeros_like(truth)).float()
+    assert torch.allclose(gated.audit_err[:n], want, rtol=1e-6, atol=0)
+    sur.close()

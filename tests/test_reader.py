@@ -94,3 +94,10 @@ def test_species_order_and_repeats(tmp_path):
     assert net.species == ["CO_1", "He", "CO_2"]  # first appearance; He already named
     with pytest.raises(ValueError, match="more than once"):
         VulcanNetwork(tmp_path / "network.txt", tmp_path / "NASA9", species=["CO_1", "CO_1", "CO_2", "He"])
+
+
+def test_condensation_lines_are_counted_whatever_their_form(tmp_path):
+    text = ("# Two-body Reactions\n1 [ H + OH -> H2 + O ] 1 0 0\n# reverse stops\n# condensation\n"
+            "5 [ H2O -> H2O_l_s ] 1 2\n6 [ not a reaction ]\n")  # fmt: skip
+    thermo = {q: invented.constant_cp(0.0) for q in ("H", "O", "OH", "H2", "He")}
+    assert invented.write(tmp_path, text, thermo).skipped == 2

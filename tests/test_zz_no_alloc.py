@@ -59,7 +59,7 @@ def test_the_static_call_matches_the_call_twice_in_a_row(gpu, networks):
         ns = plain.ns
         inp_a = inp_b = (t(w.x), t(w.T), t(w.P), t(w.dt), t(w.h), t(w.J))
         ref, got = outputs(B, ns, gpu), outputs(B, ns, gpu)
-        for k in range(2):  # a cold start cut short at MAX_STEPS tries, then a second call from its results
+        for k in range(2):  # a cold start cut short at MAX_STEPS tries, then a 1e10 s dark call from its results
             for o in (ref, got):
                 o["x"].fill_(float("nan"))
             rc, msg = c_call(lib.mx_call, plain, inp_a, ref, max_steps=MAX_STEPS)
@@ -73,8 +73,9 @@ def test_the_static_call_matches_the_call_twice_in_a_row(gpu, networks):
                 assert np.array_equal(g[name], r[name], equal_nan=True), (k, name)
             assert np.array_equal(g["total"], r["total"]), k
             assert (r["flag"] > 0).sum() == r["count"][RECOMPUTED]
-            inp_a = (ref["x"].clone(), inp_a[1], inp_a[2], inp_a[3], ref["h"].clone(), inp_a[5])
-            inp_b = (got["x"].clone(), inp_b[1], inp_b[2], inp_b[3], got["h"].clone(), inp_b[5])
+            long = torch.full_like(inp_a[3], 1e10)  # hundreds of steps: again beyond MAX_STEPS, so listed again
+            inp_a = (ref["x"].clone(), inp_a[1], inp_a[2], long, ref["h"].clone(), torch.zeros_like(inp_a[5]))
+            inp_b = (got["x"].clone(), inp_b[1], inp_b[2], long, got["h"].clone(), torch.zeros_like(inp_b[5]))
         assert static.layout()["list_cells"] == 0  # the static solver never sized a recompute list of its own
         assert plain.layout()["list_cells"] >= B
 
