@@ -172,8 +172,8 @@ int mx_call_static(mx_solver* s, const double* x, const double* T, const double*
  * M0 = I / (gamma h) - Jn is row-scaled by powers of two, factored in FP32 and every stage solve is refined `sweeps`
  * times (1..MX_MIXED_MAX_SWEEPS) against an FP64 residual formed from the rate tables (no FP64 matrix is stored);
  * rates, equilibrium constants, right-hand sides, stage vectors, the error estimate, step control and the guard stay
- * FP64. A try whose last correction exceeds tol (> 0) times the error-control scale hands its cell to the plain FP64
- * kernel, which redoes it from its inputs in the same call. Results, counts and flags have mx_call's meaning.
+ * FP64. An accepted try whose last correction exceeds tol (> 0) times the error-control scale hands its cell to the
+ * plain FP64 kernel, which redoes it from its inputs in the same call. Results, counts and flags have mx_call's meaning.
  * mx_call_static always runs the plain path.
  */
 int mx_set_precision(mx_solver* s, int32_t precision, int32_t sweeps, double tol);
@@ -386,9 +386,13 @@ int mx_destroy(mx_solver* s);
 /* The library's build identity (architecture and version), a static string. */
 const char* mx_version(void);
 
-/* Warps per cell of the call kernel: mx_network's stream groups must have 32 x that and 32 x (that - 1) threads
- * (maxichem_b200/tables.py stream_groups). No counterpart in the reference. */
+/* Warps per cell of the call kernel by default: mx_network's stream groups have 32 x that and 32 x (that - 1) threads
+ * (maxichem_b200/tables.py stream_groups). The call, recovery and mixed kernels also take 2 warps per cell (tables
+ * built for 64 and 32 threads; mx_warps_supported), which fits twice the cells per SM when registers, not shared
+ * memory, bound the occupancy; results are the same bits either way. The derivative kernels take the default only.
+ * No counterpart in the reference, whose warps per cell follow the network's size (maxichem/_constants.py:70-72). */
 int mx_warps_per_cell(void);
+int mx_warps_supported(int32_t warps);
 
 #ifdef __cplusplus
 }

@@ -176,6 +176,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     ),  # fmt: skip
     "mx_version": (ctypes.c_char_p, []),
     "mx_warps_per_cell": (ctypes.c_int, []),
+    "mx_warps_supported": (ctypes.c_int, [ctypes.c_int32]),
 }
 
 _lib: ctypes.CDLL | None = None

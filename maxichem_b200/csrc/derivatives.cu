@@ -161,6 +161,11 @@ extern "C" int mx_jvp(mx_solver* s, const double* x, const double* T, const doub
     set_error(err, errlen, "this solver was closed; build a new one");
     return MX_ERR_CLOSED;
   }
+  if (s->warps != WARPS) {
+    set_error(err, errlen, "mx_jvp: the derivative kernels take %d warps per cell; this solver's tables are for %d",
+              WARPS, s->warps);
+    return MX_ERR_NETWORK;
+  }
   if (B < 0 || B > 0x7fffffff) {
     set_error(err, errlen, "mx_jvp: B out of range: %lld", (long long)B);
     return MX_ERR_ARGUMENT;
@@ -337,6 +342,11 @@ extern "C" int mx_vjp(mx_solver* s, const double* x, const double* T, const doub
   if (!s) {
     set_error(err, errlen, "this solver was closed; build a new one");
     return MX_ERR_CLOSED;
+  }
+  if (s->warps != WARPS) {
+    set_error(err, errlen, "mx_vjp: the derivative kernels take %d warps per cell; this solver's tables are for %d",
+              WARPS, s->warps);
+    return MX_ERR_NETWORK;
   }
   if (B < 0 || B > 0x7fffffff) {
     set_error(err, errlen, "mx_vjp: B out of range: %lld", (long long)B);

@@ -27,7 +27,7 @@ enum { PH_RATES, PH_RHS_JAC, PH_LU, PH_STAGE12, PH_STAGE3, PH_STAGE4, PH_CONTROL
 // PROF: also sum clock64 cycles per phase into prof[PH_COUNT]. LIST: step only the cells a.in_list lists
 // (a.in_count[0] of them: the mixed kernel's hand-backs, or the surrogate's fallbacks), with a.in_count[1] as the queue.
 template <int W, int R, bool PROF, bool LIST = false>
-__global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const CallArgs a, long long* prof) {
+__global__ void __launch_bounds__(32 * W, 16 / W) call_kernel(const Net net, const CallArgs a, long long* prof) {
   extern __shared__ double smem[];
   const Cell c = cell_arrays(net, smem);
   const int tid = (int)threadIdx.x, nt = 32 * W, lane = tid & 31, warp = tid >> 5, ns = net.ns, ld = net.ld;
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(32 * W, 4) call_kernel(const Net net, const Ca
 // threshold pivoting, REC_STEPS times the tries, and up to REC_RETRIES retries with a smaller first try when only the
 // element test failed (recover.cuh:231-310).
 template <int W, int R>
-__global__ void __launch_bounds__(32 * W, 4) recover_kernel(const Net net, const CallArgs a, int max_steps) {
+__global__ void __launch_bounds__(32 * W, 16 / W) recover_kernel(const Net net, const CallArgs a, int max_steps) {
   const int nfl = a.count[MX_COUNT_RECOMPUTED];
   if ((int)blockIdx.x >= nfl) return;
   extern __shared__ double smem[];
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(32 * W) debug_try_kernel(const Net net, const 
 // F, Jacobian and w, LU, two-vector solve, one-vector solve, Sherman-Morrison, error, guard test. cycles[9] receives
 // the CTA-0 averages.
 template <int W, int R>
-__global__ void __launch_bounds__(32 * W, 4) time_phases_kernel(const Net net, const double* x0, double Tc, double P,
+__global__ void __launch_bounds__(32 * W, 16 / W) time_phases_kernel(const Net net, const double* x0, double Tc, double P,
                                                              double ha, const double* Jc, int reps,
                                                              long long* cycles) {
   extern __shared__ double smem[];
@@ -515,25 +515,32 @@ __global__ void __launch_bounds__(128) guard_kernel(const Net net, const double*
   flag[cell] = r;
 }
 
-template <int R>
+template <int W, int R>
 void kernels_for(mx_solver* s) {
-  s->timer = time_phases_kernel<WARPS, R>;
-  s->call = call_kernel<WARPS, R, false>;
-  s->call_prof = call_kernel<WARPS, R, true>;
-  s->call_list = call_kernel<WARPS, R, false, true>;
-  s->recover = recover_kernel<WARPS, R>;
-  s->debug = debug_try_kernel<WARPS, R>;
+  s->timer = time_phases_kernel<W, R>;
+  s->call = call_kernel<W, R, false>;
+  s->call_prof = call_kernel<W, R, true>;
+  s->call_list = call_kernel<W, R, false, true>;
+  s->recover = recover_kernel<W, R>;
+  s->debug = debug_try_kernel<W, R>;
   s->rows_per_lane = R;
 }
 
-// rows per lane of the warp solves: species up to 32, 64, 96, 128, 256
-bool pick_kernels(int ns, mx_solver* s) {
+template <int W>
+bool kernels_of(int ns, mx_solver* s) {  // rows per lane of the warp solves: species up to 32, 64, 96, 128, 256
   const int need = (ns + 31) / 32;
-  if (need <= 1) { kernels_for<1>(s); return true; }
-  if (need <= 2) { kernels_for<2>(s); return true; }
-  if (need <= 3) { kernels_for<3>(s); return true; }
-  if (need <= 4) { kernels_for<4>(s); return true; }
-  if (need <= 8) { kernels_for<8>(s); return true; }
+  if (need <= 1) { kernels_for<W, 1>(s); return true; }
+  if (need <= 2) { kernels_for<W, 2>(s); return true; }
+  if (need <= 3) { kernels_for<W, 3>(s); return true; }
+  if (need <= 4) { kernels_for<W, 4>(s); return true; }
+  if (need <= 8) { kernels_for<W, 8>(s); return true; }
+  return false;
+}
+
+// the kernels for the solver's warps per cell (2 or 4: the tables' thread streams were built for one of them)
+bool pick_kernels(int ns, mx_solver* s) {
+  if (s->warps == 4) return kernels_of<4>(ns, s);
+  if (s->warps == 2) return kernels_of<2>(ns, s);
   return false;
 }
 
@@ -612,6 +619,13 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   double etot = 0.0;
   for (int i = 0; i < ns * n->nel; i++) etot += n->atoms[i];
   net.etot = etot;
+  s->warps = n->stream_threads[0] / 32;
+  if (n->stream_threads[0] % 32 || (s->warps != 2 && s->warps != 4) || n->stream_threads[1] != 32 * (s->warps - 1)) {
+    set_error(err, errlen, "mx_create: thread streams for %d and %d threads; the kernels take 2 or 4 warps per cell "
+              "(64 and 32, or 128 and 96 threads)", n->stream_threads[0], n->stream_threads[1]);
+    delete s;
+    return MX_ERR_NETWORK;
+  }
   if (!pick_kernels(ns, s)) {
     delete s;
     return MX_ERR_NETWORK;
@@ -671,9 +685,9 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)s->call_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->call_ctas, (const void*)s->call, 32 * WARPS, s->smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->call_ctas, (const void*)s->call, 32 * s->warps, s->smem);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->recover_ctas, (const void*)s->recover, 32 * WARPS, s->smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->recover_ctas, (const void*)s->recover, 32 * s->warps, s->smem);
   if (e == cudaSuccess && (s->call_ctas < 1 || s->recover_ctas < 1)) e = cudaErrorInvalidConfiguration;
   // the tables
   std::vector<uint64_t> rx8(nr);
@@ -702,12 +716,6 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
       }
   }
   const int nsv = n->sv_ptr[ns], njt = n->jac_ptr[n->n_entries];
-  if (n->stream_threads[0] != 32 * WARPS || n->stream_threads[1] != 32 * (WARPS - 1)) {
-    set_error(err, errlen, "mx_create: the tables' thread streams are for %d and %d threads; the kernels use %d and %d",
-              n->stream_threads[0], n->stream_threads[1], 32 * WARPS, 32 * (WARPS - 1));
-    delete s;
-    return MX_ERR_NETWORK;
-  }
   if (e == cudaSuccess) e = upload(s, n->perm, ns, &net.perm);
   if (e == cudaSuccess) e = upload(s, rx8.data(), nr, &net.rx8);
   if (e == cudaSuccess) e = upload(s, n->rc, (size_t)nr * 14, &net.rc);
@@ -799,14 +807,14 @@ extern "C" int mx_call(mx_solver* s, const double* x, const double* T, const dou
       CallArgs back = a;
       back.in_list = s->sel;
       back.in_count = s->sel_count;
-      if (e == cudaSuccess) s->call_list<<<grid, 32 * WARPS, s->smem, st>>>(s->net, back, nullptr);
+      if (e == cudaSuccess) s->call_list<<<grid, 32 * s->warps, s->smem, st>>>(s->net, back, nullptr);
     } else if (s->phases) {
-      s->call_prof<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, s->phases);
+      s->call_prof<<<grid, 32 * s->warps, s->smem, st>>>(s->net, a, s->phases);
     } else {
-      s->call<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, nullptr);
+      s->call<<<grid, 32 * s->warps, s->smem, st>>>(s->net, a, nullptr);
     }
     const int rgrid = (int)std::min<int64_t>(B, (int64_t)s->recover_ctas * s->sms);
-    if (e == cudaSuccess) s->recover<<<rgrid, 32 * WARPS, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
+    if (e == cudaSuccess) s->recover<<<rgrid, 32 * s->warps, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
     if (e == cudaSuccess) e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
@@ -869,7 +877,7 @@ extern "C" int mx_guard(mx_solver* s, const double* x, double* x_out, const int3
 
 extern "C" int mx_info(const mx_solver* s, int32_t* values, int32_t n) {
   if (!s || !values) return MX_ERR_ARGUMENT;
-  const int32_t v[] = {WARPS, s->rows_per_lane, (int32_t)s->smem, s->call_ctas, s->recover_ctas, s->sms, s->net.ld,
+  const int32_t v[] = {s->warps, s->rows_per_lane, (int32_t)s->smem, s->call_ctas, s->recover_ctas, s->sms, s->net.ld,
                        s->grid_ctas < 0 ? s->call_ctas : s->grid_ctas, (int32_t)s->list_capacity,
                        (int32_t)s->mixed_smem, s->mixed_ctas, s->precision, s->sweeps};
   for (int i = 0; i < n && i < (int)(sizeof v / sizeof v[0]); i++) values[i] = v[i];
@@ -897,7 +905,7 @@ extern "C" int mx_debug_try(mx_solver* s, const double* x, double T, double P, d
                             double atol, double* out, void* stream) {
   if (!s || !x || !out || (s->net.nj > 0 && !J)) return MX_ERR_ARGUMENT;
   DeviceScope scope(s->device);
-  s->debug<<<1, 32 * WARPS, s->smem, (cudaStream_t)stream>>>(s->net, x, T, P, h, J, rtol, atol, out);
+  s->debug<<<1, 32 * s->warps, s->smem, (cudaStream_t)stream>>>(s->net, x, T, P, h, J, rtol, atol, out);
   return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
@@ -905,7 +913,7 @@ extern "C" int mx_time_phases(mx_solver* s, const double* x, double T, double P,
                               int32_t reps, int32_t ctas, int64_t* cycles, void* stream) {
   if (!s || !x || !cycles || reps < 1 || ctas < 1 || (s->net.nj > 0 && !J)) return MX_ERR_ARGUMENT;
   DeviceScope scope(s->device);
-  s->timer<<<ctas, 32 * WARPS, s->smem, (cudaStream_t)stream>>>(s->net, x, T, P, h, J, reps, (long long*)cycles);
+  s->timer<<<ctas, 32 * s->warps, s->smem, (cudaStream_t)stream>>>(s->net, x, T, P, h, J, reps, (long long*)cycles);
   return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
@@ -1033,9 +1041,9 @@ extern "C" int mx_call_static(mx_solver* s, const double* x, const double* T, co
     CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status, count,
                list, s->tries};
     const int grid = call_grid(s, B);
-    s->call<<<grid, 32 * WARPS, s->smem, st>>>(s->net, a, nullptr);
+    s->call<<<grid, 32 * s->warps, s->smem, st>>>(s->net, a, nullptr);
     const int rgrid = (int)std::min<int64_t>(B, (int64_t)s->recover_ctas * s->sms);
-    s->recover<<<rgrid, 32 * WARPS, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
+    s->recover<<<rgrid, 32 * s->warps, s->smem, st>>>(s->net, a, MX_REC_STEPS * max_steps);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
@@ -1052,3 +1060,5 @@ extern "C" int mx_call_static(mx_solver* s, const double* x, const double* T, co
 extern "C" const char* mx_version(void) { return "maxichem_b200 0.1 sm_100a"; }
 
 extern "C" int mx_warps_per_cell(void) { return WARPS; }
+
+extern "C" int mx_warps_supported(int32_t warps) { return warps == 2 || warps == 4 ? 1 : 0; }

@@ -11,7 +11,7 @@
 //
 // FP64 stays where the method needs it: rate coefficients and NASA-9 equilibrium constants, the right-hand sides,
 // the residuals, the stage vectors, the error estimate and step-size control, and the guard's element bookkeeping.
-// A try whose last refinement still moved a stage vector by more than `tol` of the error-control scale
+// An accepted try whose last refinement still moved a stage vector by more than `tol` of the error-control scale
 // (rtol |N| + atol) is not trusted: its cell is listed and redone from its inputs by the plain FP64 call kernel, which
 // mx_call launches on the listed cells right after this kernel.
 //
@@ -208,7 +208,7 @@ __device__ __forceinline__ double refine(const Net& net, const Cell& c, const Ex
 // for the plain kernel and left otherwise untouched (no output, counts or flag). LIST: step only the cells of
 // a.in_list (a.in_count[0] of them, queue a.in_count[1]), as the plain kernel's list mode.
 template <int W, int R, bool PROF, bool LIST = false>
-__global__ void __launch_bounds__(32 * W, 5)
+__global__ void __launch_bounds__(32 * W, 20 / W)
     mixed_kernel(const Net net, const CallArgs a, int sweeps, double tol, long long* prof) {
   extern __shared__ double smem[];
   const Cell c = cell_arrays(net, smem);
@@ -350,7 +350,8 @@ __global__ void __launch_bounds__(32 * W, 5)
       worst = fmax(worst, refine<R>(net, c, e, c.K4, e.B, igh, c0, a.rtol, a.atol, sweeps, tid, nt));
       if (warp == 0) {
         try_error(net, c, s.t == 0.0, a.rtol, a.atol, lane);
-        if (lane == 0) c.red[6] = (sweeps > 0 && !(worst <= tol)) ? 1.0 : 0.0;
+        // an accepted try must be trusted; a rejected one only sets the next try's size
+        if (lane == 0) c.red[6] = (sweeps > 0 && c.red[1] != 0.0 && !(worst <= tol)) ? 1.0 : 0.0;
       }
       __syncthreads();
       mark(PH_STAGE4);
@@ -549,27 +550,33 @@ __global__ void __launch_bounds__(32 * W) mixed_debug_kernel(const Net net, cons
   }
 }
 
-template <int R>
+template <int W, int R>
 void mixed_kernels_for(mx_solver* s) {
-  s->mixed = mixed_kernel<WARPS, R, false>;
-  s->mixed_prof = mixed_kernel<WARPS, R, true>;
-  s->mixed_list = mixed_kernel<WARPS, R, false, true>;
-  s->mixed_debug = mixed_debug_kernel<WARPS, R>;
+  s->mixed = mixed_kernel<W, R, false>;
+  s->mixed_prof = mixed_kernel<W, R, true>;
+  s->mixed_list = mixed_kernel<W, R, false, true>;
+  s->mixed_debug = mixed_debug_kernel<W, R>;
+}
+
+template <int W>
+bool mixed_kernels_of(mx_solver* s) {
+  switch (s->rows_per_lane) {
+    case 1: mixed_kernels_for<W, 1>(s); return true;
+    case 2: mixed_kernels_for<W, 2>(s); return true;
+    case 3: mixed_kernels_for<W, 3>(s); return true;
+    case 4: mixed_kernels_for<W, 4>(s); return true;
+    case 8: mixed_kernels_for<W, 8>(s); return true;
+    default: return false;
+  }
 }
 
 }  // namespace
 
 int mx_mixed_prepare(mx_solver* s, int n_pieces, char* err, size_t errlen) {
   const int ns = s->net.ns, nr = s->net.nr, nel = s->net.nel;
-  switch (s->rows_per_lane) {
-    case 1: mixed_kernels_for<1>(s); break;
-    case 2: mixed_kernels_for<2>(s); break;
-    case 3: mixed_kernels_for<3>(s); break;
-    case 4: mixed_kernels_for<4>(s); break;
-    case 8: mixed_kernels_for<8>(s); break;
-    default:
-      set_error(err, errlen, "mx_create: no mixed-precision kernel for %d rows per lane", s->rows_per_lane);
-      return MX_ERR_NETWORK;
+  if (!(s->warps == 4 ? mixed_kernels_of<4>(s) : mixed_kernels_of<2>(s))) {
+    set_error(err, errlen, "mx_create: no mixed-precision kernel for %d rows per lane", s->rows_per_lane);
+    return MX_ERR_NETWORK;
   }
   Net& m = s->net32;
   m = s->net;  // the tables; the layout below replaces the plain one's offsets
@@ -623,7 +630,7 @@ int mx_mixed_prepare(mx_solver* s, int n_pieces, char* err, size_t errlen) {
     e = cudaFuncSetAttribute((const void*)s->mixed_list, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)s->mixed_smem);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->mixed_ctas, (const void*)s->mixed, 32 * WARPS,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->mixed_ctas, (const void*)s->mixed, 32 * s->warps,
                                                       s->mixed_smem);
   if (e == cudaSuccess && s->mixed_ctas < 1) e = cudaErrorInvalidConfiguration;
   if (e != cudaSuccess) {
@@ -637,11 +644,11 @@ cudaError_t mx_mixed_launch(mx_solver* s, const CallArgs& a, int64_t B, bool lis
   const int per_sm = s->grid_ctas < 0 ? s->mixed_ctas : std::min(s->grid_ctas, s->mixed_ctas);
   const int grid = s->grid_ctas == 0 ? (int)B : (int)std::min<int64_t>(B, (int64_t)per_sm * s->sms);
   if (list)
-    s->mixed_list<<<grid, 32 * WARPS, s->mixed_smem, st>>>(s->net32, a, s->sweeps, s->mixed_tol, nullptr);
+    s->mixed_list<<<grid, 32 * s->warps, s->mixed_smem, st>>>(s->net32, a, s->sweeps, s->mixed_tol, nullptr);
   else if (s->phases)
-    s->mixed_prof<<<grid, 32 * WARPS, s->mixed_smem, st>>>(s->net32, a, s->sweeps, s->mixed_tol, s->phases);
+    s->mixed_prof<<<grid, 32 * s->warps, s->mixed_smem, st>>>(s->net32, a, s->sweeps, s->mixed_tol, s->phases);
   else
-    s->mixed<<<grid, 32 * WARPS, s->mixed_smem, st>>>(s->net32, a, s->sweeps, s->mixed_tol, nullptr);
+    s->mixed<<<grid, 32 * s->warps, s->mixed_smem, st>>>(s->net32, a, s->sweeps, s->mixed_tol, nullptr);
   return cudaGetLastError();
 }
 
@@ -650,7 +657,7 @@ extern "C" int mx_debug_try_mixed(mx_solver* s, const double* x, double T, doubl
   if (!s || !x || !out || (s->net.nj > 0 && !J) || sweeps < 0 || sweeps > MX_MIXED_MAX_SWEEPS) return MX_ERR_ARGUMENT;
   DeviceScope scope(s->device);
   if (scope.status != cudaSuccess) return MX_ERR_CUDA;
-  s->mixed_debug<<<1, 32 * WARPS, s->mixed_smem, (cudaStream_t)stream>>>(s->net32, x, T, P, h, J, rtol, atol, sweeps,
+  s->mixed_debug<<<1, 32 * s->warps, s->mixed_smem, (cudaStream_t)stream>>>(s->net32, x, T, P, h, J, rtol, atol, sweeps,
                                                                          out);
   return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }

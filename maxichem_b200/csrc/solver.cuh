@@ -10,7 +10,7 @@
 
 #include "device.cuh"
 
-constexpr int WARPS = 4;  // warps per cell
+constexpr int WARPS = 4;  // warps per cell by default (the derivative kernels' only mapping); the call takes 2 or 4
 
 typedef void (*CallFn)(const mx::Net, const mx::CallArgs, long long*);
 typedef void (*DebugFn)(const mx::Net, const double*, double, double, double, const double*, double, double, double*);
@@ -24,6 +24,7 @@ struct mx_derivatives;  // the tangent and adjoint kernels' state (derivatives.c
 
 struct mx_solver {
   int device = 0;
+  int warps = WARPS;  // warps per cell of the call, recovery and mixed kernels (2 or 4)
   mx::Net net{};
   std::vector<void*> buffers;
   CallFn call = nullptr;

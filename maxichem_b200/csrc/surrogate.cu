@@ -884,13 +884,13 @@ extern "C" int mx_sur_call(mx_surrogate* s, mx_solver* solver, const double* x, 
       mx::CallArgs back = a;
       back.in_list = solver->sel;
       back.in_count = solver->sel_count;
-      if (e == cudaSuccess) solver->call_list<<<grid, 32 * WARPS, solver->smem, st>>>(solver->net, back, nullptr);
+      if (e == cudaSuccess) solver->call_list<<<grid, 32 * solver->warps, solver->smem, st>>>(solver->net, back, nullptr);
     } else {
-      solver->call_list<<<grid, 32 * WARPS, solver->smem, st>>>(solver->net, a, nullptr);
+      solver->call_list<<<grid, 32 * solver->warps, solver->smem, st>>>(solver->net, a, nullptr);
     }
     const int rgrid = (int)std::min<int64_t>(B, (int64_t)solver->recover_ctas * solver->sms);
     if (e == cudaSuccess)
-      solver->recover<<<rgrid, 32 * WARPS, solver->smem, st>>>(solver->net, a, MX_REC_STEPS * max_steps);
+      solver->recover<<<rgrid, 32 * solver->warps, solver->smem, st>>>(solver->net, a, MX_REC_STEPS * max_steps);
     if (e == cudaSuccess && audit_cap > 0)
       audit_kernel<<<(audit_cap + 3) / 4, 128, 0, st>>>(audit_cells, audit_count, audit_cap, audit_x, x_out, s->ns,
                                                         audit_err);

@@ -127,11 +127,14 @@ class CudaSolver:
     Beyond the reference: ``precision`` "fp64" (the reference's arithmetic) or "mixed" (each try's linear algebra in
     row-scaled FP32, every stage solve refined ``sweeps`` times against an FP64 residual; a try whose last correction
     exceeds ``tol`` times the error-control scale has its cell redone in FP64 in the same call, counted in
-    ``escalated``). Results, counts, flags and refusals have the same meaning in both.
+    ``escalated``). Results, counts, flags and refusals have the same meaning in both. ``warps``: warps per cell of
+    the call (4 by default, or 2: more cells per SM for small networks; the same results bit for bit; the
+    derivatives need 4).
     """
 
     def __init__(self, net: VulcanNetwork, device: torch.device | str, *, drift: float | None = None,
-                 photo: bool = False, precision: str = "fp64", sweeps: int = 1, tol: float = MIXED_TOL) -> None:
+                 photo: bool = False, precision: str = "fp64", sweeps: int = 1, tol: float = MIXED_TOL,
+                 warps: int | None = None) -> None:
         self._handle: ctypes.c_void_p | None = None
         if precision not in PRECISIONS:
             raise ValueError(f"precision: one of {sorted(PRECISIONS)} expected, got {precision!r}")
@@ -151,7 +154,10 @@ class CudaSolver:
         self.net = net
         self.dev = _device_of(device)
         self._lib = abi.library()
-        self.tab = tables.build(net, photo, warps=int(self._lib.mx_warps_per_cell()))
+        self.warps = int(self._lib.mx_warps_per_cell()) if warps is None else int(warps)
+        if not self._lib.mx_warps_supported(self.warps):
+            raise ValueError(f"warps: 2 or 4 warps per cell expected, got {warps}")
+        self.tab = tables.build(net, photo, warps=self.warps)
         self.ns, self.nr, self.nj = self.tab.ns, self.tab.nr, self.tab.nj
         self.count = torch.zeros(abi.COUNT_SLOTS, dtype=torch.int32, device=self.dev)
         self.total = torch.zeros(abi.COUNT_SLOTS, dtype=torch.int64, device=self.dev)
@@ -260,9 +266,8 @@ class CudaSolver:
         queue, 0 one CTA per cell, -1 the default (the occupancy limit). Results do not depend on it."""
         self._require_open()
         if self._lib.mx_set_grid(self._handle, int(ctas_per_sm)):
-            raise ValueError(
-                f"ctas_per_sm from -1 to {self.info['call_ctas_per_sm']} expected, got {ctas_per_sm}"
-            )
+            most = max(self.info["call_ctas_per_sm"], self.info["mixed_ctas_per_sm"])
+            raise ValueError(f"ctas_per_sm from -1 to {most} expected, got {ctas_per_sm}")
         values = (ctypes.c_int32 * len(INFO_FIELDS))()
         self._lib.mx_info(self._handle, values, len(INFO_FIELDS))
         self.info["grid_ctas_per_sm"] = int(values[INFO_FIELDS.index("grid_ctas_per_sm")])

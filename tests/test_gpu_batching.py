@@ -46,8 +46,9 @@ def test_every_grid_gives_the_same_bits(uneven):
 
 def test_a_grid_beyond_the_occupancy_limit_is_refused(uneven):
     solver, _, _ = uneven
+    most = max(solver.info["call_ctas_per_sm"], solver.info["mixed_ctas_per_sm"])  # each kernel takes at most its own
     with pytest.raises(ValueError, match="ctas_per_sm from -1 to"):
-        solver.set_grid(solver.info["call_ctas_per_sm"] + 1)
+        solver.set_grid(most + 1)
     with pytest.raises(ValueError, match="ctas_per_sm from -1 to"):
         solver.set_grid(-2)
 
@@ -98,3 +99,48 @@ def test_a_captured_loop_refuses_a_cold_cell(uneven):
     loop.run(check=False)
     assert loop.refused(before) == {"bad_input": 0, "cold": 2, "hot": 0}
     loop.close()
+
+
+@pytest.mark.parametrize("name", ["cho41", "chno69", "sncho91"])
+def test_two_warps_per_cell_give_the_same_bits(gpu, networks, name):
+    net = networks(name)
+    w = synthetic.workload(net, "uneven", 1024, seed=13)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=gpu)
+    args = [t(a) for a in (w.x, w.T, w.P, w.dt, w.h)]
+    with CudaSolver(net, gpu, photo=True, warps=4) as four, CudaSolver(net, gpu, photo=True, warps=2) as two:
+        assert two.info["warps"] == 2 and four.info["warps"] == 4
+        a = four.launch(*args, J=t(w.J))
+        b = two.launch(*args, J=t(w.J))
+        assert four.fallback == two.fallback
+    for k in ("x", "h", "done", "steps", "flag"):
+        assert torch.equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_the_tuner_picks_a_mapping_and_a_grid(gpu, networks):
+    net = networks("cho41")
+    w = synthetic.workload(net, "uneven", 4096, seed=14)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=gpu)
+    args = [t(a) for a in (w.x, w.T, w.P, w.dt, w.h)]
+    solver, got = autotune.tune(net, gpu, *args, J=t(w.J))
+    assert got["warps"] in (2, 4) and solver.info["warps"] == got["warps"]
+    assert solver.info["grid_ctas_per_sm"] == got["grid"]
+    assert {k[0] for k in got["ms"]} == {2, 4}
+    r = solver.launch(*args, J=t(w.J))
+    with CudaSolver(net, gpu, photo=True) as plain:
+        assert torch.equal(plain.launch(*args, J=t(w.J)).x, r.x)
+    solver.close()
+
+
+def test_the_derivatives_refuse_two_warps(gpu, networks):
+    import ctypes
+
+    from maxichem_b200 import abi
+
+    lib = abi.library()
+    err = ctypes.create_string_buffer(256)
+    with CudaSolver(networks("cho41"), gpu, photo=True, warps=2) as two:
+        n = len(abi.SIGNATURES["mx_jvp"][1])
+        args = [two._handle] + [None] * 8 + [0, 1e-3, 1e-25, 4000, 1, 1] + [None] * 18 + [None, err, 256]
+        assert len(args) == n
+        assert lib.mx_jvp(*args) == 3  # MX_ERR_NETWORK
+    assert b"4 warps per cell" in err.value

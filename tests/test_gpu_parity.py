@@ -90,3 +90,21 @@ def test_the_sulfur_network_over_600_s_calls(gpu, networks):
         assert parity.passed_calibrated(rep, floor), (k, rep)
     assert parity.passed(reports[1][0]), reports[1][0]
 
+
+@pytest.mark.parametrize("name,dt", [("chno69", 300.0), ("sncho91", 600.0)])
+def test_a_4096_cell_sample_of_the_configuration_grid(gpu, networks, name, dt):
+    # every 16th cell of a 65,536-cell column grid (64 levels x 1,024 columns: the 69-species configuration's grid;
+    # the sulfur configuration's calls are 600 s): a cold start from solar gas, then two settling calls
+    net = networks(name)
+    full = synthetic.workload(net, "column", 65536, seed=7)
+    pick = np.arange(0, 65536, 16)
+    w = synthetic.Workload(full.x[pick], full.T[pick], full.P[pick], np.full(len(pick), dt), full.h[pick],
+                           full.J[pick])  # fmt: skip
+    reports = run_both(net, w, gpu, calls=3)
+    for k, (rep, floor) in enumerate(reports):
+        print(name, "4096-cell sample, call", k, {q: rep[q] for q in ("share_within_rtol", "worst_rel", "flips",
+                                                                        "flip_dex", "share_rel")},
+              "one-ulp floor:", {q: floor[q] for q in ("worst_rel", "share_within_rtol", "flips")})  # fmt: skip
+        assert parity.passed_calibrated(rep, floor), (k, rep)
+    for rep, _ in reports[1:]:
+        assert parity.passed(rep), rep
