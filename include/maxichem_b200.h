@@ -305,8 +305,8 @@ int mx_mole_to_mass(const double* x, const double* mw, const double* mass, int64
 
 /*
  * The learned part of the call (north-star form 4; no counterpart in the reference). A BF16 MLP surrogate of the
- * per-call solve: features of a cell (log10 x per species floored at 1e-30, log10 T, P and dt, log10(J + 1e-30) per
- * branch, standardised, zero-padded to a multiple of 64: kin) -> `layers` hidden layers of width `hidden` (SiLU) ->
+ * per-call solve: features of a cell (log10 x per species floored at 1e-30, log10 T, P, dt and the carried h,
+ * log10(J + 1e-30) per branch, standardised, zero-padded to a multiple of 64: kin) -> `layers` hidden layers of width `hidden` (SiLU) ->
  * `heads` output blocks of nt = ns + 1 values (log10 x_out - log10 x_in per species, log10 h_out; standardised),
  * padded to kout (a multiple of 64). Every layer is a tcgen05 GEMM with its bias and activation fused; training on
  * the GPU by the same GEMMs (backward dX with the SiLU derivative fused, dW), bias sums and Adam.
@@ -329,7 +329,7 @@ int mx_sur_set_scaling(mx_surrogate* s, const float* feat_mean, const float* fea
 /* Features of B cells (device inputs as mx_call's) into feat (device BF16 [B][kin]) and in_range (device int32 [B],
  * nullable: 1 when every feature is inside the training range). Asynchronous on stream. */
 int mx_sur_features(mx_surrogate* s, const double* x, const double* T, const double* P, const double* dt,
-                    const double* J, int64_t B, void* feat, int32_t* in_range, void* stream);
+                    const double* h, const double* J, int64_t B, void* feat, int32_t* in_range, void* stream);
 
 /* The network on B rows of features (device BF16 [B][kin]) into pred (device FP32 [B][kout]), in chunks of 65,536
  * rows. Asynchronous on stream. */
@@ -369,6 +369,14 @@ int mx_sur_call(mx_surrogate* s, mx_solver* solver, const double* x, const doubl
                 double* x_out, double* h_out, int32_t* done, double* steps, int32_t* flag, int32_t* status,
                 int32_t* count, int64_t* total, uint64_t* stats, int32_t* audit_cells, double* audit_x,
                 float* audit_err, int32_t* audit_count, int32_t audit_cap, void* stream, char* err, size_t errlen);
+
+/* The gate's measures without a decision (for calibrating the thresholds on held-out cells and for tests): for B
+ * cells the projected proposal into x_prop [B][ns] and, per cell, diag [B][4]: the heads' spread (dex), the
+ * projection's size (infinite when the projected proposal fails the drift test with allowance drift), 1 when the
+ * inputs are usable and inside the training range (else 0), and the proposed h. Asynchronous on stream. */
+int mx_sur_propose(mx_surrogate* s, const double* x, const double* T, const double* P, const double* dt,
+                   const double* h_in, const double* J, int64_t B, double drift, double atol, double* x_prop,
+                   double* diag, void* stream);
 
 int mx_sur_destroy(mx_surrogate* s);
 

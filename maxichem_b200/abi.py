@@ -150,7 +150,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     ),  # fmt: skip
     "mx_sur_info": (ctypes.c_int, [_P, _P, ctypes.c_int32]),
     "mx_sur_set_scaling": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
-    "mx_sur_features": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, ctypes.c_int64, _P, _P, _P]),
+    "mx_sur_features": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int64, _P, _P, _P]),
     "mx_sur_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, _P]),
     "mx_sur_train_step": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int64, ctypes.c_float, _P, _P]),
     "mx_sur_params": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.c_int64]),
@@ -163,6 +163,10 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         + [ctypes.c_int32, _P, _ERR, ctypes.c_size_t],
     ),  # fmt: skip
     "mx_sur_destroy": (ctypes.c_int, [_P]),
+    "mx_sur_propose": (
+        ctypes.c_int,
+        [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_double, ctypes.c_double, _P, _P, _P],
+    ),  # fmt: skip
     "mx_gemm_bf16": (
         ctypes.c_int,
         [_P, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -1,8 +1,8 @@
 // The learned part of the call (north-star form 4): a BF16 MLP surrogate of the per-call solve, its training on the
 // GPU, and the gated call that solves only the cells it cannot vouch for. No counterpart in the reference.
 //
-// Network: the features of a cell (log10 x per species floored at 1e-30, log10 T, P and dt, log10(J + 1e-30) per
-// branch, each standardised; zero padding to a multiple of 64) -> L hidden layers of width H with SiLU -> heads
+// Network: the features of a cell (log10 x per species floored at 1e-30, log10 T, P, dt and the carried h,
+// log10(J + 1e-30) per branch, each standardised; zero padding to a multiple of 64) -> L hidden layers of width H with SiLU -> heads
 // output blocks of (log10 x_out - log10 x_in per species, log10 h_out), standardised. Weights BF16 [out][in] (K-major
 // for the tensor cores) with FP32 master copies, biases FP32. Every layer is one tcgen05 GEMM (gemm.cuh) with its
 // bias and activation fused into the epilogue; training adds the backward GEMMs (dX with the SiLU derivative fused,
@@ -105,15 +105,17 @@ constexpr double X_FLOOR = 1e-30;  // log10 x and log10(J + floor) of the featur
 constexpr double AUDIT_FLOOR = 1e-20;  // species the audit and the spread gate judge: mole fraction above this
 
 // ---- features: one warp per cell ----
-// f = log10 x (ns, floored), log10 T, log10 P, log10 dt, log10(J + floor) (nj), zeros to kin; standardised, BF16.
-// in_range: every feature within the training set's [lo, hi] (and finite).
-__global__ void features_kernel(const double* x, const double* T, const double* P, const double* dt, const double* J,
-                                int B, int ns, int nj, int kin, const float* mean, const float* inv_std,
-                                const float* lo, const float* hi, __nv_bfloat16* feat, int* in_range) {
+// f = log10 x (ns, floored), log10 T, log10 P, log10 dt, log10 h (the carried step: how stiff and how settled the
+// cell is), log10(J + floor) (nj), zeros to kin; standardised, BF16. in_range: every feature within the training
+// set's [lo, hi] (and finite).
+__global__ void features_kernel(const double* x, const double* T, const double* P, const double* dt, const double* h,
+                                const double* J, int B, int ns, int nj, int kin, const float* mean,
+                                const float* inv_std, const float* lo, const float* hi, __nv_bfloat16* feat,
+                                int* in_range) {
   const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
   if (warp >= B) return;
   const size_t cell = (size_t)warp;
-  const int nf = ns + 3 + nj;
+  const int nf = ns + 4 + nj;
   bool inside = true;
   for (int f = lane; f < kin; f += 32) {
     double v = 0.0;
@@ -125,8 +127,10 @@ __global__ void features_kernel(const double* x, const double* T, const double* 
       v = log10(P[cell]);
     else if (f == ns + 2)
       v = log10(fmax(dt[cell], X_FLOOR));
+    else if (f == ns + 3)
+      v = log10(fmax(h[cell], X_FLOOR));
     else if (f < nf)
-      v = log10(J[cell * nj + (f - ns - 3)] + X_FLOOR);
+      v = log10(J[cell * nj + (f - ns - 4)] + X_FLOOR);
     float q = 0.0f;
     if (f < nf) {
       const float vf = (float)v;
@@ -276,6 +280,7 @@ struct GateArgs {
   int audit_cap;
   int* audit_count;
   unsigned long long* stats;  // accepted, audited, out of range, spread, projection, refused or non-finite
+  double* diag;  // propose mode: per cell the spread, the projection's size, 1 if usable and in range, the h proposal
 };
 
 __device__ __forceinline__ unsigned mix32(unsigned v) {  // an integer hash (xorshift-multiply) for the audit draw
@@ -436,6 +441,18 @@ __global__ void gate_kernel(GateArgs g) {
       drift = drift || fabs(a1s[e] / s1 - e0[e] / s0) > g.drift * e0[e] / s0 + 2.0 * g.atol * g.etot / s0;
   }
   const double hprop = exp10(log_h);
+  if (g.diag) {  // propose mode: the projected proposal of every cell and the gate's measures, nothing decided
+    double* xo = g.x_out + (size_t)cell * ns;
+    for (int i = lane; i < ns; i += 32) xo[i] = p[i];
+    if (lane == 0) {
+      double* d = g.diag + (size_t)cell * 4;
+      d[0] = spread;
+      d[1] = drift ? INFINITY : proj;
+      d[2] = (usable && in_range && isfinite(hprop)) ? 1.0 : 0.0;
+      d[3] = hprop;
+    }
+    return;
+  }
   const bool spread_ok = spread <= g.spread_max, proj_ok = proj <= g.proj_max && !drift;
   const bool accept = usable && in_range && spread_ok && proj_ok && isfinite(hprop);
   const bool audit = accept && g.audit_every > 0 && (mix32((unsigned)cell * 2654435761u ^ g.seed) % (unsigned)g.audit_every) == 0;
@@ -613,7 +630,7 @@ extern "C" int mx_sur_create(int32_t ns, int32_t nj, int32_t nel, const double* 
   s->hidden = hidden;
   s->layers = layers;
   s->heads = heads;
-  s->nf = ns + 3 + nj;
+  s->nf = ns + 4 + nj;
   s->kin = round64(s->nf);
   s->nt = ns + 1;
   s->kout = round64(heads * s->nt);
@@ -709,13 +726,14 @@ extern "C" int mx_sur_set_scaling(mx_surrogate* s, const float* feat_mean, const
 }
 
 extern "C" int mx_sur_features(mx_surrogate* s, const double* x, const double* T, const double* P, const double* dt,
-                               const double* J, int64_t B, void* feat, int32_t* in_range, void* stream) {
-  if (!s || B < 0 || B > 0x7fffffff || (B > 0 && (!x || !T || !P || !dt || !feat || (s->nj > 0 && !J))))
+                               const double* h, const double* J, int64_t B, void* feat, int32_t* in_range,
+                               void* stream) {
+  if (!s || B < 0 || B > 0x7fffffff || (B > 0 && (!x || !T || !P || !dt || !h || !feat || (s->nj > 0 && !J))))
     return MX_ERR_ARGUMENT;
   if (B == 0) return MX_OK;
   DeviceScope scope(s->device);
   const int threads = 256, blocks = (int)((B * 32 + threads - 1) / threads);
-  features_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(x, T, P, dt, J, (int)B, s->ns, s->nj, s->kin,
+  features_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(x, T, P, dt, h, J, (int)B, s->ns, s->nj, s->kin,
                                                                 s->fmean, s->finv, s->flo, s->fhi,
                                                                 (__nv_bfloat16*)feat, in_range);
   return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
@@ -863,7 +881,7 @@ extern "C" int mx_sur_call(mx_surrogate* s, mx_solver* solver, const double* x, 
     return MX_ERR_CUDA;
   }
   if (B > 0) {
-    rc = mx_sur_features(s, x, T, P, dt, J, B, s->cfeat, s->in_range, stream);
+    rc = mx_sur_features(s, x, T, P, dt, h_in, J, B, s->cfeat, s->in_range, stream);
     if (!rc) rc = mx_sur_forward(s, s->cfeat, B, s->cpred, stream);
     if (rc) {
       set_error(err, errlen, "mx_sur_call: the network's forward pass failed (%d)", rc);
@@ -872,7 +890,7 @@ extern "C" int mx_sur_call(mx_surrogate* s, mx_solver* solver, const double* x, 
     GateArgs g{x, T, dt, h_in, (int)B, s->ns, s->nel, s->nt, s->heads, s->kout, s->cpred, s->tmean, s->tstd,
                s->in_range, s->atoms, spread_max, proj_max, solver->net.drift, atol, s->etot, audit_every, seed,
                x_out, h_out, steps, done, flag, status, count, s->list, s->list_count, audit_cells, audit_x,
-               audit_cap, audit_count, (unsigned long long*)stats};
+               audit_cap, audit_count, (unsigned long long*)stats, nullptr};
     const int warps = 4, gsmem = warps * (s->ns + MX_MAX_ELEMENTS * MX_MAX_ELEMENTS + 4 * MX_MAX_ELEMENTS + 4) * 8;
     gate_kernel<<<(int)((B + warps - 1) / warps), 32 * warps, gsmem, st>>>(g);
     // the Rodas3 fallback on the listed cells, then the recovery of what its guard listed
@@ -905,6 +923,26 @@ extern "C" int mx_sur_call(mx_surrogate* s, mx_solver* solver, const double* x, 
     return MX_ERR_CUDA;
   }
   return MX_OK;
+}
+
+extern "C" int mx_sur_propose(mx_surrogate* s, const double* x, const double* T, const double* P, const double* dt,
+                              const double* h_in, const double* J, int64_t B, double drift, double atol,
+                              double* x_prop, double* diag, void* stream) {
+  if (!s || B < 0 || B > 0x7fffffff || !(drift >= 0.0) || !(atol > 0.0) ||
+      (B > 0 && (!x || !T || !P || !dt || !h_in || !x_prop || !diag || (s->nj > 0 && !J))))
+    return MX_ERR_ARGUMENT;
+  if (B == 0) return MX_OK;
+  DeviceScope scope(s->device);
+  if (grow_call(s, B) != cudaSuccess) return MX_ERR_CUDA;
+  int rc = mx_sur_features(s, x, T, P, dt, h_in, J, B, s->cfeat, s->in_range, stream);
+  if (!rc) rc = mx_sur_forward(s, s->cfeat, B, s->cpred, stream);
+  if (rc) return rc;
+  GateArgs g{x, T, dt, h_in, (int)B, s->ns, s->nel, s->nt, s->heads, s->kout, s->cpred, s->tmean, s->tstd,
+             s->in_range, s->atoms, 0.0, 0.0, drift, atol, s->etot, 0, 0u, x_prop, nullptr, nullptr, nullptr,
+             nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, diag};
+  const int warps = 4, gsmem = warps * (s->ns + MX_MAX_ELEMENTS * MX_MAX_ELEMENTS + 4 * MX_MAX_ELEMENTS + 4) * 8;
+  gate_kernel<<<(int)((B + warps - 1) / warps), 32 * warps, gsmem, (cudaStream_t)stream>>>(g);
+  return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
 extern "C" int mx_sur_destroy(mx_surrogate* s) {

@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from . import abi, synthetic
-from .constants import ATOL, DEFAULT_MAX_STEPS, DEFAULT_RTOL
+from .constants import ATOL, DEFAULT_MAX_STEPS, DEFAULT_RTOL, DRIFT
 from .solver import CallResult, CudaSolver, check_inputs, check_photolysis
 
 _ERRLEN = 1024
@@ -45,10 +45,11 @@ def quantile(v: torch.Tensor, q: float) -> float:
     return float(s[lo] + (s[hi] - s[lo]) * (pos - lo))
 
 
-def raw_features(x: torch.Tensor, T: torch.Tensor, P: torch.Tensor, dt: torch.Tensor, J: torch.Tensor | None) -> torch.Tensor:
+def raw_features(x: torch.Tensor, T: torch.Tensor, P: torch.Tensor, dt: torch.Tensor, h: torch.Tensor,
+                 J: torch.Tensor | None) -> torch.Tensor:
     """The features before standardisation, as the library's features kernel forms them (FP32 [B][nf])."""
     cols = [torch.log10(x.clamp_min(X_FLOOR)), torch.log10(T)[:, None], torch.log10(P)[:, None],
-            torch.log10(dt.clamp_min(X_FLOOR))[:, None]]  # fmt: skip
+            torch.log10(dt.clamp_min(X_FLOOR))[:, None], torch.log10(h.clamp_min(X_FLOOR))[:, None]]  # fmt: skip
     if J is not None and J.shape[1]:
         cols.append(torch.log10(J + X_FLOOR))
     return torch.cat(cols, 1).float()
@@ -198,16 +199,31 @@ class Surrogate:
         if rc:
             raise ValueError("mx_sur_set_scaling refused the scaling")
 
-    def features(self, x, T, P, dt, J) -> tuple[torch.Tensor, torch.Tensor]:
+    def features(self, x, T, P, dt, h, J) -> tuple[torch.Tensor, torch.Tensor]:
         B = x.shape[0]
         feat = torch.empty(B, self.kin, dtype=torch.bfloat16, device=self.dev)
         inr = torch.empty(B, dtype=torch.int32, device=self.dev)
         stream = torch.cuda.current_stream(self.dev).cuda_stream
         rc = self._lib.mx_sur_features(self._handle, x.data_ptr(), T.data_ptr(), P.data_ptr(), dt.data_ptr(),
-                                       None if J is None else J.data_ptr(), B, feat.data_ptr(), inr.data_ptr(), stream)  # fmt: skip
+                                       h.data_ptr(), None if J is None else J.data_ptr(), B, feat.data_ptr(),
+                                       inr.data_ptr(), stream)  # fmt: skip
         if rc:
             raise RuntimeError(f"mx_sur_features failed ({rc})")
         return feat, inr
+
+    def propose(self, x, T, P, dt, h, J, *, drift: float = DRIFT, atol: float = ATOL) -> tuple[torch.Tensor, torch.Tensor]:
+        """The gate's projected proposal of every cell [B][ns] and its measures [B][4]: spread (dex), projection size
+        (inf on drift), 1 when usable and in range, proposed h (mx_sur_propose)."""
+        B = x.shape[0]
+        xp = torch.empty(B, self.ns, dtype=torch.float64, device=self.dev)
+        diag = torch.empty(B, 4, dtype=torch.float64, device=self.dev)
+        stream = torch.cuda.current_stream(self.dev).cuda_stream
+        rc = self._lib.mx_sur_propose(self._handle, x.data_ptr(), T.data_ptr(), P.data_ptr(), dt.data_ptr(),
+                                      h.data_ptr(), None if J is None else J.data_ptr(), B, float(drift), float(atol),
+                                      xp.data_ptr(), diag.data_ptr(), stream)  # fmt: skip
+        if rc:
+            raise RuntimeError(f"mx_sur_propose failed ({rc})")
+        return xp, diag
 
     def forward(self, feat: torch.Tensor) -> torch.Tensor:
         pred = torch.empty(feat.shape[0], self.kout, dtype=torch.float32, device=self.dev)
@@ -239,10 +255,10 @@ class Surrogate:
             log: list | None = None) -> dict[str, Any]:
         """Train on `data`: standardisation from the data, each head on its own Poisson(1) bootstrap weights, Adam with
         a cosine decay from lr. Returns the loss per epoch."""
-        raw = raw_features(data.x, data.T, data.P, data.dt, data.J)
+        raw = raw_features(data.x, data.T, data.P, data.dt, data.h, data.J)
         tgt = targets(data.x, data.x_out, data.h_out)
         self.set_scaling(raw, tgt)
-        feat, _ = self.features(data.x, data.T, data.P, data.dt, data.J)
+        feat, _ = self.features(data.x, data.T, data.P, data.dt, data.h, data.J)
         y = self.standardised_targets(tgt)
         gen = torch.Generator(device=self.dev)
         gen.manual_seed(seed)
@@ -286,39 +302,28 @@ class Surrogate:
         self._push_scaling()
 
 
-def calibrate(sur: Surrogate, data: Pairs, target: float = 1e-3, quantile_: float = 0.999) -> dict[str, float]:
-    """The spread threshold (dex) of the gate: the largest one under which the accepted cells of `data` (held out from
-    training) have their per-species relative error (species above 1e-20) within `target` at `quantile`. Returns it
-    with the share of cells it accepts."""
-    feat, inr = sur.features(data.x, data.T, data.P, data.dt, data.J)
-    hd = sur.heads_of(sur.forward(feat)).double()
-    mu = hd.mean(1)
-    sd = hd.std(1)
-    ns = sur.ns
-    prop = 10.0 ** (torch.log10(data.x.clamp_min(X_FLOOR)) + mu[:, :ns])
-    prop = prop / prop.sum(1, keepdim=True)
-    judged = torch.maximum(data.x, prop) > AUDIT_FLOOR
-    spread = torch.where(judged, sd[:, :ns], torch.zeros_like(sd[:, :ns])).amax(1)
-    big = data.x_out > AUDIT_FLOOR
-    rel = torch.where(big, (prop - data.x_out).abs() / data.x_out.clamp_min(1e-300), torch.zeros_like(prop))
+def calibrate(sur: "Surrogate", data: Pairs, *, target: float = 1e-3, quantile_: float = 0.999,
+              proj_max: float = 1e-2, margin: float = 0.5, drift: float = DRIFT, atol: float = ATOL) -> dict[str, float]:
+    """The gate's spread threshold from held-out pairs (not trained on): accepting eligible cells (inputs usable and in
+    range, projection at most proj_max, drift test passed) in order of increasing spread, the largest threshold under
+    which the call's per-species relative error against the plain solver (over every cell and species above 1e-20;
+    a rejected cell carries Rodas3's result, error 0) stays within `target` at `quantile_`, with only `margin` of the
+    allowed share of values beyond it spent. Returns {"spread_max", "proj_max", "accept"} (accept: the share of
+    `data`'s cells the threshold accepts; spread_max 0 when none can be)."""
+    xp, diag = sur.propose(data.x, data.T, data.P, data.dt, data.h, data.J, drift=drift, atol=atol)
+    truth = data.x_out
+    big = truth > AUDIT_FLOOR
+    err = torch.where(big, (xp - truth).abs() / truth.clamp_min(1e-300), torch.zeros_like(truth))
+    bad = (err > target).sum(1).double()
+    budget = (1.0 - quantile_) * float(big.sum()) * margin
+    eligible = (diag[:, 2] == 1) & (diag[:, 1] <= proj_max)
+    spread = torch.where(eligible, diag[:, 0], torch.full_like(diag[:, 0], math.inf))
     order = torch.argsort(spread)
-    s_sorted, e_sorted, inr_sorted = spread[order], rel[order], inr[order].bool()
-    best = {"spread_max": 0.0, "accept": 0.0}
-    lo, hi = 0, len(order)
-    while lo < hi:  # the largest prefix whose errors meet the target
-        mid = (lo + hi + 1) // 2
-        keep = inr_sorted[:mid]
-        errs = e_sorted[:mid][keep]
-        bigs = big[order][:mid][keep]
-        vals = errs[bigs]
-        ok = vals.numel() == 0 or quantile(vals, quantile_) <= target
-        if ok:
-            lo = mid
-        else:
-            hi = mid - 1
-    if lo > 0:
-        best = {"spread_max": float(s_sorted[lo - 1]), "accept": float(inr_sorted[:lo].sum()) / len(order)}
-    return best
+    fine = (torch.cumsum(bad[order], 0) <= budget) & torch.isfinite(spread[order])
+    k = int(fine.long().cumprod(0).sum())  # the longest admissible prefix
+    if k == 0:
+        return {"spread_max": 0.0, "proj_max": proj_max, "accept": 0.0}
+    return {"spread_max": float(spread[order[k - 1]]), "proj_max": proj_max, "accept": k / len(data)}
 
 
 class GatedSolver:
@@ -371,6 +376,24 @@ class GatedSolver:
         out = self.launch_raw(x, T, P, dt, h, rtol=rtol, atol=atol, max_steps=max_steps, J=jx)
         s._refuse(x, T, P, dt, jx, out["status"])
         s.flag = out["flag"]
+        return CallResult(out["x"], out["h"], out["done"].bool(), out["steps"])
+
+    def call_host(self, x, T, P, dt, h, *, rtol=DEFAULT_RTOL, atol=ATOL, max_steps=DEFAULT_MAX_STEPS, J=None,
+                  out: dict[str, torch.Tensor] | None = None) -> CallResult:
+        """The gated call on host (CPU) tensors: the inputs copied to the device, the call, the outputs copied back
+        (into `out`'s pinned host tensors x, h, steps, done, flag, status when given), one stream, one synchronisation
+        for the refusal check."""
+        s = self.solver
+        dev = s.dev
+        ins = [torch.as_tensor(a).to(dev, non_blocking=True) for a in (x, T, P, dt, h)]
+        jd = None if J is None else torch.as_tensor(J).to(dev, non_blocking=True)
+        r = self.launch_raw(*ins, rtol=rtol, atol=atol, max_steps=max_steps, J=jd)
+        if out is None:
+            out = {k: torch.empty(v.shape, dtype=v.dtype).pin_memory() for k, v in r.items()}
+        for k, v in r.items():
+            out[k].copy_(v, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        s._refuse(*ins[:4], jd, r["status"])
         return CallResult(out["x"], out["h"], out["done"].bool(), out["steps"])
 
     def counts(self) -> dict[str, int]:

@@ -34,17 +34,17 @@ def small(gpu, networks):
 def test_features_are_the_standardised_logs(small, gpu):
     net, solver, data = small
     sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, hidden=128, layers=2, heads=2)
-    raw = sg.raw_features(data.x, data.T, data.P, data.dt, data.J)
+    raw = sg.raw_features(data.x, data.T, data.P, data.dt, data.h, data.J)
     sur.set_scaling(raw, sg.targets(data.x, data.x_out, data.h_out))
-    feat, inr = sur.features(data.x, data.T, data.P, data.dt, data.J)
+    feat, inr = sur.features(data.x, data.T, data.P, data.dt, data.h, data.J)
     sc = sur.scaling
     want = (raw.cpu().numpy() - sc["fmean"]) / np.where(sc["fstd"] > 0, sc["fstd"], 1.0)
     got = feat.float().cpu().numpy()
     assert np.abs(got[:, : sur.nf] - ref.bf16(want)).max() <= 2**-7 * np.abs(want).max()
     assert (got[:, sur.nf :] == 0).all() and bool(inr.bool().all())
     shifted = data.T.clone()
-    shifted[:5] = 10.0 ** (sc["fhi"][solver.ns] + 0.01)  # T above the training range
-    _, inr2 = sur.features(data.x, shifted, data.P, data.dt, data.J)
+    shifted[:5] = float(10.0 ** (float(sc["fhi"][solver.ns]) + 0.01))  # T above the training range
+    _, inr2 = sur.features(data.x, shifted, data.P, data.dt, data.h, data.J)
     assert not bool(inr2[:5].bool().any()) and bool(inr2[5:].bool().all())
     sur.close()
 
@@ -52,11 +52,11 @@ def test_features_are_the_standardised_logs(small, gpu):
 def test_gradients_match_the_cpu_reference_layer_by_layer(small, gpu):
     net, solver, data = small
     sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, seed=3)  # 4 x 512, 4 heads
-    raw = sg.raw_features(data.x, data.T, data.P, data.dt, data.J)
+    raw = sg.raw_features(data.x, data.T, data.P, data.dt, data.h, data.J)
     tg = sg.targets(data.x, data.x_out, data.h_out)
     sur.set_scaling(raw, tg)
     M = 256
-    feat, _ = sur.features(data.x[:M], data.T[:M], data.P[:M], data.dt[:M], data.J[:M])
+    feat, _ = sur.features(data.x[:M], data.T[:M], data.P[:M], data.dt[:M], data.h[:M], data.J[:M])
     y = sur.standardised_targets(tg[:M])
     wts = torch.poisson(torch.ones(M, sur.heads, device=gpu)).float()
     p0 = sur.params()
@@ -131,4 +131,23 @@ def test_accepted_cells_conserve_and_audited_cells_are_solved(small, gpu):
     prop, truth = gated.audit_x[:n], plain.x[cells]
     want = torch.where(truth > sg.AUDIT_FLOOR, (prop - truth).abs() / truth, torch.zeros_like(truth)).float()
     assert torch.allclose(gated.audit_err[:n], want, rtol=1e-6, atol=0)
+    sur.close()
+
+
+def test_the_gate_decides_on_the_proposals_measures(small, gpu):
+    net, solver, data = small
+    sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, seed=11)
+    sur.fit(data, epochs=3, batch=1024)
+    n = 2048
+    args = (data.x_out[:n] / data.x_out[:n].sum(1, keepdim=True), data.T[:n], data.P[:n], data.dt[:n], data.h_out[:n])
+    J = data.J[:n]
+    xp, diag = sur.propose(*args, J, drift=solver.drift)
+    spread_max = float(torch.quantile(diag[:, 0][diag[:, 2] == 1], 0.5))
+    gated = sg.GatedSolver(solver, sur, spread_max=spread_max, proj_max=0.05, audit_every=0)
+    r = gated(*args, J=J)
+    want = (diag[:, 2] == 1) & (diag[:, 0] <= spread_max) & (diag[:, 1] <= 0.05)
+    acc = (r.steps == 0) & r.done
+    assert torch.equal(acc, want) and int(want.sum()) > 0
+    assert torch.equal(r.x[acc], xp[acc])
+    assert gated.counts()["accepted"] == int(want.sum())
     sur.close()
