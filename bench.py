@@ -23,6 +23,7 @@ import sys
 import threading
 import time
 from pathlib import Path
+from typing import Any
 
 import numpy as np
 
@@ -60,6 +61,11 @@ def parse() -> argparse.Namespace:
                    help="time the call with its tangent (jvp, --directions of them) or its adjoint (vjp) instead")
     p.add_argument("--directions", type=int, default=1, help="tangent directions of --derivative jvp")
     p.add_argument("--frozen", action="store_true", help="--derivative with adapt=False (the accepted steps held)")
+    p.add_argument("--arms", default="fp64,learned",
+                   help="comma list of fp64, learned (the surrogate's gated call), mixed (FP32 factors)")
+    p.add_argument("--train-cells", type=int, default=1 << 20, help="cells of the surrogate's training pairs")
+    p.add_argument("--train-calls", type=int, default=6, help="chained calls of the training pairs")
+    p.add_argument("--epochs", type=int, default=20, help="training epochs of the surrogate")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -194,10 +200,78 @@ def main() -> None:
     if args.derivative:
         run_derivative(args)
         return
+    run_call(args)
+
+
+def timed_steps(fn, steps: int, warmup: int, stream) -> tuple[float, Any]:
+    """W untimed calls, then K calls between CUDA events on the launching stream: ms per call and the last output."""
+    import torch
+
+    out = None
+    for _ in range(warmup):
+        out = fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, out
+
+
+def accuracy(ref: dict, got: dict) -> dict:
+    """Per-species relative error of `got`'s x against the plain FP64 call's (species above 1e-20), over the call."""
+    import torch
+
+    from maxichem_b200.surrogate import quantile
+
+    big = ref["x"] > 1e-20
+    rel = ((got["x"] - ref["x"]).abs() / ref["x"])[big]
+    rel = torch.nan_to_num(rel, nan=float("inf"))
+    return {"p50": quantile(rel, 0.5), "p99": quantile(rel, 0.99), "p999": quantile(rel, 0.999),
+            "max": float(rel.max()), "share_above_rtol": float((rel > 1e-3).double().mean()),
+            "done_all": bool(got["done"].bool().all())}  # fmt: skip
+
+
+def train_surrogate(solver, args, dev) -> tuple[Any, dict]:
+    """The learned part, trained on the GPU by the library's kernels on pairs from the plain solver (other cells than
+    the timed ones: the uneven column workload, seeds 2000/3000), its gate calibrated on held-out pairs."""
+    from maxichem_b200 import surrogate as sg
+
+    t0 = time.perf_counter()
+    train = sg.pairs(solver, args.train_cells, args.train_calls, seed=2000, cold_share=0.1, dt=args.dt)
+    val = sg.pairs(solver, 131072, args.train_calls, seed=3000, cold_share=0.1, dt=args.dt)
+    gen_s = time.perf_counter() - t0
+    sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, dev, seed=1)
+    t0 = time.perf_counter()
+    fit = sur.fit(train, epochs=args.epochs, batch=16384, lr=2e-3)
+    torch_sync()
+    fit_s = time.perf_counter() - t0
+    cal = max((sg.calibrate(sur, val, target=1e-3, proj_max=pm) for pm in (1e-3, 1e-2, 1e-1)),
+              key=lambda c: c["accept"])  # fmt: skip
+    info = {"pairs": len(train), "held_out": len(val), "generate_s": round(gen_s, 2), "fit_s": round(fit_s, 2),
+            "epochs": args.epochs, "final_loss": fit["loss"][-1], "adam_steps": fit["steps"], "calibration": cal,
+            "network": f"{sur.kin} -> {sur.layers} x {sur.hidden} SiLU -> {sur.heads} heads x {sur.nt} (BF16)"}  # fmt: skip
+    return sur, info
+
+
+def torch_sync() -> None:
+    import torch
+
+    torch.cuda.synchronize()
+
+
+def run_call(args) -> None:
+    """The call on 1,048,576 cells of the settled column grid, by arm: "fp64" (the plain Rodas3 path), "learned" (the
+    BF16 surrogate's gated call with the FP64 path solving what it rejects, and a 1/64 audit), "mixed" (FP32 factors
+    with FP64 refinement). The headline value is the fastest arm whose call meets the bar against the FP64 arm's
+    result on the same inputs (per-species error within rtol 1e-3 at the 99.9th percentile, every cell done)."""
     import torch
     import torch.distributed as dist
 
     from maxichem_b200 import abi, replicas, synthetic
+    from maxichem_b200 import surrogate as sg
     from maxichem_b200.solver import CudaSolver, check_inputs
 
     rank, local, world = replicas.rank_from_env()
@@ -207,11 +281,12 @@ def main() -> None:
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    arms = [a for a in args.arms.split(",") if a]
     net = synthetic.network(args.network)
     B = args.cells
     w = inputs(net, B, seed=replicas.seed(1000, rank))  # each rank its own batch of columns (weak scaling)
     w.dt[:] = args.dt
-    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)  # noqa: E731
     solver = CudaSolver(net, dev, photo=True)
     tab = solver.tab
     x, T, P, dt, h, J = t(w.x), t(w.T), t(w.P), t(w.dt), t(w.h), t(w.J)
@@ -221,82 +296,136 @@ def main() -> None:
         x, h, _, steps = solver(x, T, P, dt, h, J=J)
         spin.append({"s": round(time.perf_counter() - t0, 3), "steps_mean": float(steps.mean())})
     check_inputs(dev, tab.ns, x, T, P, dt, h, 1e-3, 1e-25, 4000)
-    tries = torch.zeros(3, dtype=torch.int64, device=dev)
     lib = abi.library()
-    lib.mx_set_try_counter(solver._handle, tries.data_ptr())
-    out = None
-    for _ in range(args.warmup):
-        out = solver.launch_raw(x, T, P, dt, h, rtol=1e-3, atol=1e-25, max_steps=4000, J=J, out=out)
-    torch.cuda.synchronize(dev)
-    tries.zero_()
     stream = torch.cuda.current_stream(dev)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
+    kw = dict(rtol=1e-3, atol=1e-25, max_steps=4000, J=J)
+    report: dict[str, Any] = {}
+    runners: dict[str, Any] = {}
+    gated = sur_info = mixed = None
+    if "learned" in arms:
+        sur, sur_info = train_surrogate(solver, args, dev)
+        cal = sur_info["calibration"]
+        gated = sg.GatedSolver(solver, sur, spread_max=cal["spread_max"], proj_max=cal["proj_max"], audit_every=64,
+                               seed=7)  # fmt: skip
+        runners["learned"] = lambda: gated.launch_raw(x, T, P, dt, h, **kw)  # noqa: E731
+    if "mixed" in arms:
+        mixed = CudaSolver(net, dev, photo=True, precision="mixed")
+        runners["mixed"] = lambda: mixed.launch_raw(x, T, P, dt, h, **kw)  # noqa: E731
+    tries = torch.zeros(3, dtype=torch.int64, device=dev)
+    lib.mx_set_try_counter(solver._handle, tries.data_ptr())
+    outs: dict[str, Any] = {}
     with Clocks(local) as clocks:
-        e_all0 = torch.cuda.Event(enable_timing=True)
-        e_all1 = torch.cuda.Event(enable_timing=True)
-        e_all0.record(stream)
-        for k in range(args.steps):
-            starts[k].record(stream)
-            out = solver.launch_raw(x, T, P, dt, h, rtol=1e-3, atol=1e-25, max_steps=4000, J=J, out=out)
-            ends[k].record(stream)
-        e_all1.record(stream)
+        if world > 1:
+            dist.barrier()
         torch.cuda.synchronize(dev)
-    total_ms = replicas.max_over_ranks(e_all0.elapsed_time(e_all1), dev)  # the slowest rank's device time
-    if world > 1:
-        dist.barrier()
-    ms = total_ms / args.steps
-    counts = replicas.sum_counts(solver.count).cpu().tolist()  # every rank's cells
-    nt = tries.cpu().tolist()
+        ms64, outs["fp64"] = timed_steps(lambda: solver.launch_raw(x, T, P, dt, h, **kw), args.steps, args.warmup,
+                                         stream)  # fmt: skip
+        nt = tries.cpu().tolist()
+        tries.zero_()
+        report["fp64"] = {"ms_per_step": replicas.max_over_ranks(ms64, dev), "counts": solver.fallback,
+                          "fresh_tries": nt[0] - nt[1], "retries": nt[1]}  # fmt: skip
+        for arm, fn in runners.items():
+            if gated is not None and arm == "learned":
+                gated.stats.zero_()
+            steps_arm = args.steps if arm != "mixed" else max(1, min(args.steps, 3))
+            ms, outs[arm] = timed_steps(fn, steps_arm, min(args.warmup, 3), stream)
+            report[arm] = {"ms_per_step": replicas.max_over_ranks(ms, dev), "steps": steps_arm,
+                           "accuracy_vs_fp64": accuracy(outs["fp64"], outs[arm])}  # fmt: skip
+        if world > 1:
+            dist.barrier()
+    lib.mx_set_try_counter(solver._handle, None)
+    if gated is not None:
+        n_calls = args.steps + min(args.warmup, 3)
+        c = gated.counts()
+        report["learned"].update(
+            {"accepted_share": c["accepted"] / (n_calls * B), "audit": gated.audit(), "surrogate": sur_info,
+             "gate_counts_per_call": {k: v / n_calls for k, v in c.items()}, "counts": solver.fallback,
+             "cpu_reads_per_call": 0})  # fmt: skip
+    if mixed is not None:
+        report["mixed"]["escalated_per_call"] = int(mixed.escalated.item()) / (report["mixed"]["steps"] + 3)
+        report["mixed"]["counts"] = mixed.fallback
+    for arm in report:
+        report[arm]["cells_per_s"] = replicas.throughput(B, world, report[arm]["ms_per_step"] * 1e-3)
+    bar = lambda r: ("accuracy_vs_fp64" not in r or  # noqa: E731
+                     (r["accuracy_vs_fp64"]["p999"] <= 1e-3 and r["accuracy_vs_fp64"]["done_all"]))
+    headline = max((a for a in report if bar(report[a])), key=lambda a: report[a]["cells_per_s"])
+    ms = report[headline]["ms_per_step"]
+    value = report[headline]["cells_per_s"]
+    counts = replicas.sum_counts(solver.total).cpu().tolist()
     phases = phase_shares(solver, lib, x, T, P, dt, h, J, dev)
-    steps_mean = float(out["steps"].mean())
-    value = replicas.throughput(B, world, ms * 1e-3)
-    # roofline: algorithmic FP64 work of the call kernel per launch / its time (events on the launching stream)
+    steps_mean = float(outs["fp64"]["steps"].mean())
+    # roofline: the FP64 call kernel, the dominant kernel of every arm (the learned arm's fallback is this kernel on
+    # the cells the gate rejects): algorithmic FP64 work of its tries / the plain arm's time per call
     f = tab.flops
-    fresh, retry = nt[0] - nt[1], nt[1]
-    flop_step = (fresh * f["fresh_try"] + retry * f["retry"] + B * f["rates"]) / args.steps
+    fresh, retry = report["fp64"]["fresh_tries"], report["fp64"]["retries"]
+    flop_step = (fresh * f["fresh_try"] + retry * f["retry"] + (args.steps + args.warmup) * B * f["rates"]) / (
+        args.steps + args.warmup)
     peak = ctypes_probe(lib, local)
-    achieved = flop_step / (ms * 1e-3) / 1e12
-    # the call's HBM I/O: x, T, P, dt, h, J in; x, h, steps (f64) and done, flag, status (int32) out
+    achieved = flop_step / (report["fp64"]["ms_per_step"] * 1e-3) / 1e12
     io_bytes = B * (8 * (2 * tab.ns + tab.nj + 6) + 12)
     line = {
         "metric": METRIC if (args.network, args.dt) == (NETWORK, DT) else
                   f"cells/s per GCM call ({tab.ns}-sp, {B * world} cells, dt {args.dt:g} s): FP64 Rodas3",
         "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded 69-species network and column grid; the VULCAN networks are absent)",
+        "dtype": "f64" if headline == "fp64" else ("bf16+f64" if headline == "learned" else "f32+f64"),
+        "data": "synthetic (seeded 69-species network and column grid; the VULCAN networks are absent)",
         "config": {"workload": f"{args.network}: call {SPINUP_CALLS + 1} of {args.dt:g} s calls on a {LEVELS}-level "
                                "column grid",
+                   "headline_arm": headline, "arms": report,
                    "cells_per_gpu": B, "species": tab.ns, "reactions": tab.nr, "photolysis": tab.nj,
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
-                   "accepted_steps_mean": steps_mean, "tries_per_cell": nt[0] / args.steps / B,
-                   "retries_per_cell": nt[1] / args.steps / B, "recovery_tries": nt[2] / args.steps,
+                   "accepted_steps_mean": steps_mean, "tries_per_cell": (fresh + retry) / (args.steps + args.warmup) / B,
                    "counts": dict(zip(["queue", *abi_counts()], counts)), "spinup": spin, "layout": solver.info,
                    "phase_shares": phases},
-        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak / 1e3, "unit": "TFLOP/s",
-                     "frac": achieved / (peak / 1e3) if peak else None, "traffic": TRAFFIC_PER_CELL * B,
+        "roofline": {"bound": "fp64", "kernel": "call_kernel (the plain arm)", "achieved": achieved,
+                     "peak": peak / 1e3, "unit": "TFLOP/s", "frac": achieved / (peak / 1e3) if peak else None,
+                     "traffic": TRAFFIC_PER_CELL * B,
                      "traffic_source": "ncu DRAM bytes of the call kernel at 262,144 cells, scaled by cells",
-                     "algorithmic_bytes": io_bytes, "hbm_gbs": io_bytes / (ms * 1e-3) / 1e9,
-                     "hbm_frac_of_measured": io_bytes / (ms * 1e-3) / 1e9 / HBM_GBS,
+                     "algorithmic_bytes": io_bytes, "hbm_gbs": io_bytes / (report["fp64"]["ms_per_step"] * 1e-3) / 1e9,
+                     "hbm_frac_of_measured": io_bytes / (report["fp64"]["ms_per_step"] * 1e-3) / 1e9 / HBM_GBS,
                      "peak_source": "measured in-process: FP64 fma chains on every SM (mx_probe_fp64)",
                      "flops_per_step": flop_step},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": 3 * args.steps + (86 * args.steps if "learned" in report else 0),
         "clocks": clocks.summary(),
     }  # fmt: skip
+    if gated is not None:
+        line["roofline_mlp"] = mlp_roofline(gated.sur, x, T, P, dt, h, J, stream)
     if not args.no_e2e:
-        line["e2e"] = e2e(solver, x, h, w, dev, args)
+        if headline == "learned":
+            line["e2e"] = e2e_gated(gated, x, h, w, dev, args)
+        else:
+            line["e2e"] = e2e(solver, x, h, w, dev, args)
         line["e2e"]["ms_per_step"] = replicas.max_over_ranks(line["e2e"]["ms_per_step"], dev)
         line["e2e"]["value"] = replicas.throughput(B, world, line["e2e"]["ms_per_step"] * 1e-3)
+        line["e2e"]["arm"] = headline
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(tab, x, h, w, args)
+    if gated is not None:
+        gated.sur.close()
+    if mixed is not None:
+        mixed.close()
     solver.close()
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def mlp_roofline(sur, x, T, P, dt, h, J, stream) -> dict:
+    """The surrogate network's forward pass on the timed cells: its tcgen05 GEMMs' FLOPs over their time, against the
+    measured sustained BF16 peak."""
+    import torch
+
+    feat, _ = sur.features(x, T, P, dt, h, J)
+    ms, _ = timed_steps(lambda: sur.forward(feat), 5, 2, stream)
+    flop = 2.0 * feat.shape[0] * sum(r * c for r, c in sur.shapes)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("bf16_tflops_sustained", 1400.0)
+    torch.cuda.synchronize()
+    return {"bound": "tensor", "kernel": "gemm_kernel (the network's 5 layers)", "achieved": flop / ms / 1e9,
+            "peak": peak, "unit": "TFLOP/s", "frac": flop / ms / 1e9 / peak, "ms_per_forward": ms,
+            "flops_per_forward": flop, "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained"}  # fmt: skip
 
 
 def run_derivative(args) -> None:
@@ -499,6 +628,26 @@ def e2e(solver, x, h, w, dev, args) -> dict:
     d2h = sum(a.numel() * a.element_size() for a in (ox, oh, odone, ost, oflag, ostatus))
     return {"value": hx.shape[0] / (ms * 1e-3), "unit": "cells/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": ms}  # fmt: skip
+
+
+def e2e_gated(gated, x, h, w, dev, args) -> dict:
+    """The learned arm through its public API from pinned host buffers (GatedSolver.call_host): H2D of x, T, P, dt, h,
+    J, the gated call with its refusal check, D2H of x, h, steps, done, flag, status."""
+    import torch
+
+    pin = lambda a: torch.as_tensor(a, dtype=torch.float64).pin_memory()  # noqa: E731
+    hx, hT, hP, hdt, hh, hJ = (pin(a) for a in (x.cpu(), w.T, w.P, w.dt, h.cpu(), w.J))
+    B = hx.shape[0]
+    out = {"x": torch.empty_like(hx).pin_memory(), "h": torch.empty_like(hh).pin_memory(),
+           "steps": torch.empty_like(hh).pin_memory(),
+           **{k: torch.empty(B, dtype=torch.int32).pin_memory() for k in ("done", "flag", "status")}}  # fmt: skip
+    stream = torch.cuda.current_stream(dev)
+    ms, _ = timed_steps(lambda: gated.call_host(hx, hT, hP, hdt, hh, J=hJ, out=out), args.steps, max(1, args.warmup),
+                        stream)  # fmt: skip
+    h2d = sum(a.numel() * a.element_size() for a in (hx, hT, hP, hdt, hh, hJ))
+    d2h = sum(a.numel() * a.element_size() for a in out.values())
+    return {"value": B / (ms * 1e-3), "unit": "cells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": ms}  # fmt: skip
 
 
 def cpu_baseline(tab, x, h, w, args) -> dict:

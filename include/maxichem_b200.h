@@ -337,10 +337,11 @@ int mx_sur_forward(mx_surrogate* s, const void* feat, int64_t B, float* pred, vo
 
 /* One Adam step (lr, betas 0.9 / 0.999, eps 1e-8) on a batch of M rows (a multiple of 64): features feat (BF16
  * [M][kin]), standardised targets tgt (FP32 [M][nt]) and per-row head weights wts (FP32 [M][heads], the heads'
- * bootstrap draw). The loss is the weighted mean square error over rows, heads and targets; *loss (device FP32,
- * nullable) is incremented by it. Asynchronous on stream; lr 0 computes the gradients only (mx_sur_params 1). */
+ * bootstrap draw). The loss is the weighted mean over rows, heads and targets of the square error (delta 0) or of
+ * the Huber loss of width delta (> 0, in standardised units); *loss (device FP32, nullable) is incremented by it.
+ * Asynchronous on stream; lr 0 computes the gradients only (mx_sur_params 1). */
 int mx_sur_train_step(mx_surrogate* s, const void* feat, const float* tgt, const float* wts, int64_t M, float lr,
-                      float* loss, void* stream);
+                      float delta, float* loss, void* stream);
 
 /* The FP32 parameters (which 0) or the last step's gradients (which 1) into a host array of P floats, layer by layer:
  * W_l [out][in] then b_l [out]. Synchronises. mx_sur_set_params writes them (and restarts Adam). */

@@ -152,7 +152,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "mx_sur_set_scaling": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "mx_sur_features": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_int64, _P, _P, _P]),
     "mx_sur_forward": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P, _P]),
-    "mx_sur_train_step": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int64, ctypes.c_float, _P, _P]),
+    "mx_sur_train_step": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int64, ctypes.c_float, ctypes.c_float, _P, _P]),
     "mx_sur_params": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.c_int64]),
     "mx_sur_set_params": (ctypes.c_int, [_P, _P, ctypes.c_int64]),
     "mx_sur_error": (ctypes.c_int, [_P, _P]),

@@ -1,12 +1,11 @@
 // A BF16 GEMM on the 5th-generation tensor cores of sm_100a, with the epilogues of the surrogate network.
 //
-// C[M, N] = A[M, K] B[N, K]^T, A and B row-major BF16 (both K-major), FP32 accumulation in tensor memory. One CTA of
-// 128 threads computes a 128 x BN tile: thread 0 streams the K blocks of A and B into a ring of shared-memory stages
-// with TMA (128-byte swizzle, tensor maps over this GPU's memory only), thread 32 issues the tcgen05.mma's (M 128, N BN,
-// K 16 each, four per 64-wide K block) into a TMEM accumulator of BN columns and hands each stage back to the producer
-// with tcgen05.commit; then all four warps read the accumulator (tcgen05.ld 32x32b, warp w the rows 32w..32w+31),
-// apply the epilogue and store. Every wait on an mbarrier gives up after about a second of clock ticks: the CTA then
-// sets *err, lets its issued copies and MMAs finish (bounded waits), frees its tensor memory and returns.
+// C[M, N] = A[M, K] B[N, K]^T, A and B row-major BF16 (both K-major), FP32 accumulation in tensor memory, in tiles of
+// 128 x BN: TMA streams the K blocks of A and B into shared-memory stages (128-byte swizzle, tensor maps over this
+// GPU's memory only), one thread issues the tcgen05.mma's (M 128, N BN, K 16 each, four per 64-wide K block) into a
+// TMEM accumulator and hands each stage back with tcgen05.commit, and four warps read the accumulator (tcgen05.ld
+// 32x32b) through the epilogue. Every wait on an mbarrier gives up after about a second of clock ticks: the CTA then
+// sets *err, lets its issued copies finish (bounded waits), frees its tensor memory and returns.
 //
 // Epilogues: STORE (C in FP32), BIAS (C + bias in FP32), BIAS_SILU (z = C + bias, optionally kept in FP32; the BF16
 // output silu(z) = z sigmoid(z)), DSILU (the backward of SiLU: BF16 C * silu'(z) with z read in FP32).
@@ -115,37 +114,96 @@ __device__ __forceinline__ void tmem_load16(uint32_t taddr, uint32_t (&v)[16]) {
 
 __device__ __forceinline__ float sigmoid(float z) { return 1.0f / (1.0f + __expf(-z)); }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 // Shared-memory bytes of one CTA: the stages (1024-aligned), the barriers and the TMEM address slot, plus the slack
 // that aligns the dynamic base to 1024 bytes.
 template <int BN, int STAGES>
 __host__ __device__ constexpr int gemm_smem_bytes() {
-  return STAGES * (BM + BN) * BK * 2 + 8 * (2 * STAGES + 1) + 16 + 1024;
+  return STAGES * (BM + BN) * BK * 2 + 8 * (2 * STAGES + 4) + 16 + 1024;
 }
 
+// The epilogue of 16 accumulator columns of one row (a[16]): columns col .. col + 15 of row `row`.
+__device__ __forceinline__ void epilogue16(const Epi& ep, float (&a)[16], int row, int col) {
+  if (ep.mode == STORE || ep.mode == BIAS) {
+    if (ep.mode == BIAS)
+#pragma unroll
+      for (int j = 0; j < 16; j++) a[j] += ep.bias[col + j];
+    float4* o = (float4*)((float*)ep.out + (size_t)row * ep.ldo + col);
+#pragma unroll
+    for (int j = 0; j < 4; j++) o[j] = make_float4(a[4 * j], a[4 * j + 1], a[4 * j + 2], a[4 * j + 3]);
+    return;
+  }
+  if (ep.mode == BIAS_SILU) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) a[j] += ep.bias[col + j];
+    if (ep.z) {
+      float4* zo = (float4*)(ep.z + (size_t)row * ep.ldz + col);
+#pragma unroll
+      for (int j = 0; j < 4; j++) zo[j] = make_float4(a[4 * j], a[4 * j + 1], a[4 * j + 2], a[4 * j + 3]);
+    }
+#pragma unroll
+    for (int j = 0; j < 16; j++) a[j] = a[j] * sigmoid(a[j]);
+  } else {  // DSILU
+    const float4* zi = (const float4*)(ep.z + (size_t)row * ep.ldz + col);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const float4 z4 = zi[j];
+      const float zz[4] = {z4.x, z4.y, z4.z, z4.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float sg = sigmoid(zz[q]);
+        a[4 * j + q] *= sg * (1.0f + zz[q] * (1.0f - sg));
+      }
+    }
+  }
+  uint32_t packed[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const __nv_bfloat162 p = __floats2bfloat162_rn(a[2 * j], a[2 * j + 1]);
+    packed[j] = *reinterpret_cast<const uint32_t*>(&p);
+  }
+  uint4* o = (uint4*)((__nv_bfloat16*)ep.out + (size_t)row * ep.ldo + col);
+  o[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+  o[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+}
+
+// Persistent and warp-specialised: one CTA of 6 warps per SM walks the output tiles (row tiles outer, column tiles
+// inner, so neighbouring tiles share A's rows in L2). Warp 0 (one thread) streams the K blocks of A and B into a ring
+// of STAGES shared-memory stages; warp 1 (one thread) issues the MMAs into one of two TMEM accumulators of BN columns
+// each and commits; warps 2-5 drain the other accumulator (warp w the TMEM lanes 32 (w % 4) ..) through the epilogue
+// and hand it back, so a tile's epilogue overlaps the next tile's MMAs.
 template <int BN, int STAGES>
-__global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ CUtensorMap ta,
-                                                      const __grid_constant__ CUtensorMap tb, int M, int K, Epi ep,
-                                                      int* err) {
+__global__ void __launch_bounds__(192, 1) gemm_kernel(const __grid_constant__ CUtensorMap ta,
+                                                      const __grid_constant__ CUtensorMap tb, int M, int N, int K,
+                                                      Epi ep, int* err) {
   extern __shared__ uint8_t gemm_smem_raw[];
   uint8_t* base = (uint8_t*)(((uintptr_t)gemm_smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t* sa = base;                                 // STAGES x [128][64] BF16
-  uint8_t* sb = base + STAGES * BM * BK * 2;          // STAGES x [BN][64] BF16
-  uint64_t* bars = (uint64_t*)(sb + STAGES * BN * BK * 2);  // full[STAGES], empty[STAGES], done
-  uint32_t* tslot = (uint32_t*)(bars + 2 * STAGES + 1);
+  uint8_t* sa = base;                                        // STAGES x [128][64] BF16
+  uint8_t* sb = base + STAGES * BM * BK * 2;                 // STAGES x [BN][64] BF16
+  uint64_t* bars = (uint64_t*)(sb + STAGES * BN * BK * 2);   // full[S], empty[S], acc_full[2], acc_empty[2]
+  uint32_t* tslot = (uint32_t*)(bars + 2 * STAGES + 4);
   const int tid = (int)threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = (int)blockIdx.x * BM, n0 = (int)blockIdx.y * BN, nk = K / BK;
-  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES), done = smem_u32(bars + 2 * STAGES);
+  const int nk = K / BK, tiles_n = N / BN, tiles = ((M + BM - 1) / BM) * tiles_n;
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
+  const uint32_t accf0 = smem_u32(bars + 2 * STAGES), acce0 = smem_u32(bars + 2 * STAGES + 2);
   if (tid == 0) {
     for (int s = 0; s < STAGES; s++) {
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
     }
-    mbar_init(done, 1);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, 4);  // one arrival per epilogue warp
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  if (warp == 0) {  // the accumulator: BN columns of tensor memory (a power of two >= 32)
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(BN)
+  if (warp == 1) {  // two accumulators of BN columns (2 BN a power of two >= 32, at most 512)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(2 * BN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -153,97 +211,83 @@ __global__ void __launch_bounds__(128, 1) gemm_kernel(const __grid_constant__ CU
   __syncthreads();
   tmem_fence_after();
   const uint32_t tmem = *tslot;
-  if (tid == 0) {  // producer
+  if (warp == 0 && lane == 0) {  // producer
     int issued_round[STAGES];
     for (int s = 0; s < STAGES; s++) issued_round[s] = -1;
-    for (int kb = 0; kb < nk; kb++) {
-      const int s = kb % STAGES, r = kb / STAGES;
-      if (r > 0 && !mbar_wait(empty0 + 8 * s, (uint32_t)((r - 1) & 1), err)) break;
-      mbar_expect_tx(full0 + 8 * s, (uint32_t)((BM + BN) * BK * 2));
-      tma_load_2d(smem_u32(sa + s * BM * BK * 2), &ta, full0 + 8 * s, kb * BK, m0);
-      tma_load_2d(smem_u32(sb + s * BN * BK * 2), &tb, full0 + 8 * s, kb * BK, n0);
-      issued_round[s] = r;
+    long long kc = 0;
+    bool ok = true;
+    for (int t = (int)blockIdx.x; t < tiles && ok; t += (int)gridDim.x) {
+      const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+      for (int kb = 0; kb < nk; kb++, kc++) {
+        const int s = (int)(kc % STAGES), r = (int)(kc / STAGES);
+        if (r > 0 && !mbar_wait(empty0 + 8 * s, (uint32_t)((r - 1) & 1), err)) {
+          ok = false;
+          break;
+        }
+        mbar_expect_tx(full0 + 8 * s, (uint32_t)((BM + BN) * BK * 2));
+        tma_load_2d(smem_u32(sa + s * BM * BK * 2), &ta, full0 + 8 * s, kb * BK, m0);
+        tma_load_2d(smem_u32(sb + s * BN * BK * 2), &tb, full0 + 8 * s, kb * BK, n0);
+        issued_round[s] = r;
+      }
     }
     for (int s = 0; s < STAGES; s++)  // the copies this thread issued have landed before the CTA may exit
       if (issued_round[s] >= 0) mbar_wait(full0 + 8 * s, (uint32_t)(issued_round[s] & 1), err);
-  } else if (tid == 32) {  // MMA issuer
+  } else if (warp == 1 && lane == 0) {  // MMA issuer
     constexpr uint32_t idesc = bf16_idesc(BN);
-    for (int kb = 0; kb < nk; kb++) {
-      const int s = kb % STAGES, r = kb / STAGES;
-      if (!mbar_wait(full0 + 8 * s, (uint32_t)(r & 1), err)) break;
+    long long kc = 0;
+    bool ok = true;
+    int i = 0;
+    for (int t = (int)blockIdx.x; t < tiles && ok; t += (int)gridDim.x, i++) {
+      const int acc = i & 1, use = i >> 1;
+      if (use > 0 && !mbar_wait(acce0 + 8 * acc, (uint32_t)((use - 1) & 1), err)) break;
       tmem_fence_after();
-      const uint64_t da = sw128_desc(smem_u32(sa + s * BM * BK * 2));
-      const uint64_t db = sw128_desc(smem_u32(sb + s * BN * BK * 2));
-#pragma unroll
-      for (int k = 0; k < BK / 16; k++)  // +32 bytes along K within the swizzled 128-byte rows: +2 in 16-byte units
-        umma_bf16(tmem, da + 2 * k, db + 2 * k, idesc, (kb > 0 || k > 0) ? 1u : 0u);
-      umma_commit(empty0 + 8 * s);
-    }
-    umma_commit(done);  // fires when every MMA issued above has completed
-  }
-  __syncwarp();
-  // epilogue: warp w reads accumulator rows (TMEM lanes) 32w .. 32w + 31, one row per thread
-  const bool ready = mbar_wait(done, 0u, err);
-  tmem_fence_after();
-  const int row = m0 + 32 * warp + lane;
-  if (ready) {
-#pragma unroll 1
-    for (int c = 0; c < BN; c += 16) {
-      uint32_t v[16];
-      tmem_load16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c, v);
-      if (row >= M) continue;
-      const int col = n0 + c;
-      float a[16];
-#pragma unroll
-      for (int j = 0; j < 16; j++) a[j] = __uint_as_float(v[j]);
-      if (ep.mode == STORE || ep.mode == BIAS) {
-        if (ep.mode == BIAS)
-#pragma unroll
-          for (int j = 0; j < 16; j++) a[j] += ep.bias[col + j];
-        float4* o = (float4*)((float*)ep.out + (size_t)row * ep.ldo + col);
-#pragma unroll
-        for (int j = 0; j < 4; j++) o[j] = make_float4(a[4 * j], a[4 * j + 1], a[4 * j + 2], a[4 * j + 3]);
-      } else {
-        if (ep.mode == BIAS_SILU) {
-#pragma unroll
-          for (int j = 0; j < 16; j++) a[j] += ep.bias[col + j];
-          if (ep.z) {
-            float4* zo = (float4*)(ep.z + (size_t)row * ep.ldz + col);
-#pragma unroll
-            for (int j = 0; j < 4; j++) zo[j] = make_float4(a[4 * j], a[4 * j + 1], a[4 * j + 2], a[4 * j + 3]);
-          }
-#pragma unroll
-          for (int j = 0; j < 16; j++) a[j] = a[j] * sigmoid(a[j]);
-        } else {  // DSILU
-          const float4* zi = (const float4*)(ep.z + (size_t)row * ep.ldz + col);
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const float4 z4 = zi[j];
-            const float zz[4] = {z4.x, z4.y, z4.z, z4.w};
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-              const float sg = sigmoid(zz[q]);
-              a[4 * j + q] *= sg * (1.0f + zz[q] * (1.0f - sg));
-            }
-          }
+      const uint32_t d = tmem + (uint32_t)(acc * BN);
+      for (int kb = 0; kb < nk; kb++, kc++) {
+        const int s = (int)(kc % STAGES), r = (int)(kc / STAGES);
+        if (!mbar_wait(full0 + 8 * s, (uint32_t)(r & 1), err)) {
+          ok = false;
+          break;
         }
-        uint32_t packed[8];
+        tmem_fence_after();
+        const uint64_t da = sw128_desc(smem_u32(sa + s * BM * BK * 2));
+        const uint64_t db = sw128_desc(smem_u32(sb + s * BN * BK * 2));
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-          const __nv_bfloat162 p = __floats2bfloat162_rn(a[2 * j], a[2 * j + 1]);
-          packed[j] = *reinterpret_cast<const uint32_t*>(&p);
-        }
-        uint4* o = (uint4*)((__nv_bfloat16*)ep.out + (size_t)row * ep.ldo + col);
-        o[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-        o[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        for (int k = 0; k < BK / 16; k++)  // +32 bytes along K within the swizzled 128-byte rows: +2 in 16-byte units
+          umma_bf16(d, da + 2 * k, db + 2 * k, idesc, (kb > 0 || k > 0) ? 1u : 0u);
+        umma_commit(empty0 + 8 * s);
       }
+      umma_commit(accf0 + 8 * acc);  // fires when this tile's MMAs (and every earlier one) have completed
+    }
+  } else if (warp >= 2) {  // epilogue: warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31, one row per thread
+    const int quarter = warp & 3;
+    int i = 0;
+    for (int t = (int)blockIdx.x; t < tiles; t += (int)gridDim.x, i++) {
+      const int acc = i & 1, use = i >> 1;
+      const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+      if (!mbar_wait(accf0 + 8 * acc, (uint32_t)(use & 1), err)) break;
+      tmem_fence_after();
+      const int row = m0 + 32 * quarter + lane;
+#pragma unroll 1
+      for (int c = 0; c < BN; c += 16) {
+        uint32_t v[16];
+        tmem_load16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(acc * BN + c), v);
+        if (row < M) {
+          float a[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++) a[j] = __uint_as_float(v[j]);
+          epilogue16(ep, a, row, n0 + c);
+        }
+      }
+      tmem_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce0 + 8 * acc);
     }
   }
   tmem_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 1) {
     tmem_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
   }
 }
 

@@ -53,6 +53,8 @@ bool tensor_map(CUtensorMap* m, const void* p, uint64_t rows, uint64_t cols, uin
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+int g_sms = 0;
+
 template <int BN, int STAGES>
 cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int N, int K, const Epi& ep, int* err,
                         cudaStream_t st) {
@@ -64,8 +66,14 @@ cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M,
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  const dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)(N / BN));
-  gemm_kernel<BN, STAGES><<<grid, 128, smem, st>>>(ta, tb, (int)M, K, ep, err);
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const long long tiles = ((M + BM - 1) / BM) * (long long)(N / BN);
+  const int grid = (int)std::min<long long>(tiles, std::max(g_sms, 1));  // persistent: one CTA per SM
+  gemm_kernel<BN, STAGES><<<grid, 192, smem, st>>>(ta, tb, (int)M, N, K, ep, err);
   return cudaGetLastError();
 }
 
@@ -80,13 +88,14 @@ int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, in
       ((ep.mode == BIAS || ep.mode == BIAS_SILU) && !ep.bias) || (ep.mode == DSILU && !ep.z))
     return MX_ERR_ARGUMENT;
   if (encoder() != cudaSuccess) return MX_ERR_CUDA;
-  const bool wide = N % 128 == 0;
+  const int bn = N % 256 == 0 ? 256 : (N % 128 == 0 ? 128 : 64);  // the widest column tile that divides N
   CUtensorMap ta, tb;
   if (!tensor_map(&ta, A, (uint64_t)M, (uint64_t)K, (uint64_t)lda, BM) ||
-      !tensor_map(&tb, B, (uint64_t)N, (uint64_t)K, (uint64_t)ldb, wide ? 128 : 64))
+      !tensor_map(&tb, B, (uint64_t)N, (uint64_t)K, (uint64_t)ldb, (uint32_t)bn))
     return MX_ERR_ARGUMENT;
-  const cudaError_t e = wide ? launch_tile<128, 3>(ta, tb, M, N, K, ep, err, st)
-                             : launch_tile<64, 4>(ta, tb, M, N, K, ep, err, st);
+  const cudaError_t e = bn == 256   ? launch_tile<256, 4>(ta, tb, M, N, K, ep, err, st)
+                        : bn == 128 ? launch_tile<128, 6>(ta, tb, M, N, K, ep, err, st)
+                                    : launch_tile<64, 8>(ta, tb, M, N, K, ep, err, st);
   return e == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
@@ -145,10 +154,13 @@ __global__ void features_kernel(const double* x, const double* T, const double* 
 
 // ---- training: the loss's gradient at the heads, transposes, bias sums, Adam ----
 
-// dpred = 2 w (pred - tgt) / (M heads nt) (standardised targets, per-sample bootstrap weight w of each head), BF16,
-// zero in the padding columns; *loss += the weighted mean square error (for reports).
+// The gradient of the weighted loss at the heads, BF16, zero in the padding columns (standardised targets, per-sample
+// bootstrap weight w of each head): for delta 0 the mean square error, dpred = 2 w (pred - tgt) / (M heads nt); for
+// delta > 0 the Huber loss of width delta (quadratic within delta, linear beyond, so the few large misses of far
+// from settled cells do not outweigh the many small ones the gate must get right): dpred = 2 w clamp(pred - tgt,
+// -delta, delta) / (M heads nt). *loss += the weighted loss (for reports).
 __global__ void loss_grad_kernel(const float* pred, int ldp, const float* tgt, const float* wts, int M, int nt,
-                                 int heads, int kout, __nv_bfloat16* dpred, float* loss) {
+                                 int heads, int kout, float delta, __nv_bfloat16* dpred, float* loss) {
   __shared__ float part[256];
   const float scale = 1.0f / ((float)M * (float)heads * (float)nt);
   float acc = 0.0f;
@@ -160,8 +172,13 @@ __global__ void loss_grad_kernel(const float* pred, int ldp, const float* tgt, c
     if (head < heads) {
       const float d = pred[(size_t)row * ldp + col] - tgt[(size_t)row * nt + i];
       const float w = wts[(size_t)row * heads + head];
-      g = 2.0f * w * d * scale;
-      acc += w * d * d;
+      if (delta > 0.0f && fabsf(d) > delta) {
+        g = 2.0f * w * copysignf(delta, d) * scale;
+        acc += w * delta * (2.0f * fabsf(d) - delta);
+      } else {
+        g = 2.0f * w * d * scale;
+        acc += w * d * d;
+      }
     }
     dpred[(size_t)row * kout + col] = __float2bfloat16_rn(g);
   }
@@ -754,8 +771,9 @@ extern "C" int mx_sur_forward(mx_surrogate* s, const void* feat, int64_t B, floa
 }
 
 extern "C" int mx_sur_train_step(mx_surrogate* s, const void* feat, const float* tgt, const float* wts, int64_t M,
-                                 float lr, float* loss, void* stream) {
-  if (!s || !feat || !tgt || !wts || M < 64 || M % 64 || M > 0x7fffffff || !(lr >= 0.0f)) return MX_ERR_ARGUMENT;
+                                 float lr, float delta, float* loss, void* stream) {
+  if (!s || !feat || !tgt || !wts || M < 64 || M % 64 || M > 0x7fffffff || !(lr >= 0.0f) || !(delta >= 0.0f))
+    return MX_ERR_ARGUMENT;
   DeviceScope scope(s->device);
   cudaStream_t st = (cudaStream_t)stream;
   if (grow_train(s, M) != cudaSuccess) return MX_ERR_CUDA;
@@ -763,7 +781,7 @@ extern "C" int mx_sur_train_step(mx_surrogate* s, const void* feat, const float*
   int rc = forward(s, f, M, s->pred, true, st);
   if (rc) return rc;
   loss_grad_kernel<<<blocks_for(M * s->kout, 256), 256, 0, st>>>(s->pred, s->kout, tgt, wts, (int)M, s->nt, s->heads,
-                                                                  s->kout, s->dz, loss);
+                                                                  s->kout, delta, s->dz, loss);
   __nv_bfloat16 *dZ = s->dz, *dZ2 = s->dz2;
   int N = s->kout;
   for (int l = s->layers; l >= 0; l--) {

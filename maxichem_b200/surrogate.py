@@ -184,11 +184,17 @@ class Surrogate:
             off += rows
         return out
 
-    def set_scaling(self, raw: torch.Tensor, tgt: torch.Tensor) -> None:
-        """Standardisation and training range from raw features [N][nf] and unstandardised targets [N][nt]."""
+    def set_scaling(self, raw: torch.Tensor, tgt: torch.Tensor, target_scale: float | None = None) -> None:
+        """Standardisation and training range from raw features [N][nf] and unstandardised targets [N][nt]; the
+        targets' scale is their deviation, or one fixed `target_scale` (dex) for all of them with no shift."""
         f = raw.double()
+        t = tgt.double()
+        if target_scale is None:
+            tmean, tstd = t.mean(0), t.std(0).clamp_min(STD_FLOOR)
+        else:
+            tmean, tstd = torch.zeros_like(t[0]), torch.full_like(t[0], float(target_scale))
         sc = {"fmean": f.mean(0), "fstd": f.std(0), "flo": f.min(0).values, "fhi": f.max(0).values,
-              "tmean": tgt.double().mean(0), "tstd": tgt.double().std(0).clamp_min(STD_FLOOR)}  # fmt: skip
+              "tmean": tmean, "tstd": tstd}  # fmt: skip
         self.scaling = {k: v.float().cpu().numpy() for k, v in sc.items()}
         self._push_scaling()
 
@@ -233,10 +239,10 @@ class Surrogate:
         return pred
 
     def train_step(self, feat: torch.Tensor, tgt: torch.Tensor, wts: torch.Tensor, lr: float,
-                   loss: torch.Tensor | None = None) -> None:
+                   loss: torch.Tensor | None = None, delta: float = 0.0) -> None:
         stream = torch.cuda.current_stream(self.dev).cuda_stream
         rc = self._lib.mx_sur_train_step(self._handle, feat.data_ptr(), tgt.data_ptr(), wts.data_ptr(), feat.shape[0],
-                                         float(lr), None if loss is None else loss.data_ptr(), stream)  # fmt: skip
+                                         float(lr), float(delta), None if loss is None else loss.data_ptr(), stream)  # fmt: skip
         if rc:
             raise ValueError(f"mx_sur_train_step refused the batch ({rc}): rows a multiple of 64 expected")
 
@@ -252,12 +258,13 @@ class Surrogate:
         return ((tgt - m) / s).float().contiguous()
 
     def fit(self, data: Pairs, *, epochs: int = 8, batch: int = 8192, lr: float = 2e-3, seed: int = 0,
-            log: list | None = None) -> dict[str, Any]:
-        """Train on `data`: standardisation from the data, each head on its own Poisson(1) bootstrap weights, Adam with
-        a cosine decay from lr. Returns the loss per epoch."""
+            target_scale: float | None = None, delta: float = 0.0, log: list | None = None) -> dict[str, Any]:
+        """Train on `data`: standardisation from the data (the targets' own deviations, or one fixed `target_scale` in
+        dex), each head on its own Poisson(1) bootstrap weights, the square error (delta 0) or the Huber loss of
+        width delta, Adam with a cosine decay from lr. Returns the loss per epoch."""
         raw = raw_features(data.x, data.T, data.P, data.dt, data.h, data.J)
         tgt = targets(data.x, data.x_out, data.h_out)
-        self.set_scaling(raw, tgt)
+        self.set_scaling(raw, tgt, target_scale)
         feat, _ = self.features(data.x, data.T, data.P, data.dt, data.h, data.J)
         y = self.standardised_targets(tgt)
         gen = torch.Generator(device=self.dev)
@@ -275,7 +282,7 @@ class Surrogate:
             for b in range(0, n, batch):
                 idx = order[b : b + batch]
                 rate = lr * 0.5 * (1.0 + math.cos(math.pi * k / steps))
-                self.train_step(feat[idx].contiguous(), y[idx].contiguous(), wts[idx].contiguous(), rate, loss)
+                self.train_step(feat[idx].contiguous(), y[idx].contiguous(), wts[idx].contiguous(), rate, loss, delta)
                 k += 1
             history.append(float(loss.item()) / (n // batch))
             if log is not None:

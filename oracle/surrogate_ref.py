@@ -50,16 +50,24 @@ def forward(feat: np.ndarray, layers: list[tuple[np.ndarray, np.ndarray]]) -> tu
     return (a[-1] @ bf16(w).T + b).astype(FLOAT), a, z
 
 
-def loss_grad(pred: np.ndarray, tgt: np.ndarray, wts: np.ndarray, heads: int, nt: int) -> tuple[np.ndarray, float]:
-    """The heads' gradient (BF16 values, padding columns 0) and the weighted mean square error."""
+def loss_grad(pred: np.ndarray, tgt: np.ndarray, wts: np.ndarray, heads: int, nt: int,
+              delta: float = 0.0) -> tuple[np.ndarray, float]:
+    """The heads' gradient (BF16 values, padding columns 0) and the weighted loss: the mean square error (delta 0) or
+    the Huber loss of width delta (quadratic within it, linear beyond)."""
     M = pred.shape[0]
     d = np.zeros_like(pred)
     loss = 0.0
     scale = 1.0 / (M * heads * nt)
     for h in range(heads):
         diff = pred[:, h * nt : (h + 1) * nt] - tgt
-        d[:, h * nt : (h + 1) * nt] = 2.0 * wts[:, h : h + 1] * diff * scale
-        loss += float((wts[:, h : h + 1] * diff * diff).sum()) * scale
+        w = wts[:, h : h + 1]
+        if delta > 0:
+            clipped = np.clip(diff, -delta, delta)
+            value = np.where(np.abs(diff) > delta, delta * (2.0 * np.abs(diff) - delta), diff * diff)
+        else:
+            clipped, value = diff, diff * diff
+        d[:, h * nt : (h + 1) * nt] = 2.0 * w * clipped * scale
+        loss += float((w * value).sum()) * scale
     return bf16(d), loss
 
 

@@ -49,7 +49,8 @@ def test_features_are_the_standardised_logs(small, gpu):
     sur.close()
 
 
-def test_gradients_match_the_cpu_reference_layer_by_layer(small, gpu):
+@pytest.mark.parametrize("delta", [0.0, 0.5])
+def test_gradients_match_the_cpu_reference_layer_by_layer(small, gpu, delta):
     net, solver, data = small
     sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, seed=3)  # 4 x 512, 4 heads
     raw = sg.raw_features(data.x, data.T, data.P, data.dt, data.h, data.J)
@@ -61,13 +62,13 @@ def test_gradients_match_the_cpu_reference_layer_by_layer(small, gpu):
     wts = torch.poisson(torch.ones(M, sur.heads, device=gpu)).float()
     p0 = sur.params()
     loss = torch.zeros(1, dtype=torch.float32, device=gpu)
-    sur.train_step(feat, y, wts, 0.0, loss)  # lr 0: the gradients alone
+    sur.train_step(feat, y, wts, 0.0, loss, delta)  # lr 0: the gradients alone (square error, or Huber)
     sur.check()
     gpu_grads = sur.unpack(sur.params(1))
     assert np.array_equal(sur.params(), p0)
     layers = ref.unpack(p0, sur.shapes)
     pred, a, z = ref.forward(feat.float().cpu().numpy(), layers)
-    dpred, lossr = ref.loss_grad(pred, y.cpu().numpy(), wts.cpu().numpy(), sur.heads, sur.nt)
+    dpred, lossr = ref.loss_grad(pred, y.cpu().numpy(), wts.cpu().numpy(), sur.heads, sur.nt, delta)
     grads = ref.backward(dpred, layers, a, z)
     assert abs(float(loss.item()) - lossr) <= 1e-3 * lossr
     for l, ((gw, gb), (rw, rb)) in enumerate(zip(gpu_grads, grads)):

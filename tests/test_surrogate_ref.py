@@ -3,6 +3,7 @@ taken out, its backward pass equals central differences of its own loss, layer b
 round-to-nearest-even on the top 16 bits."""
 
 import numpy as np
+import pytest
 
 from oracle import surrogate_ref as ref
 
@@ -13,7 +14,8 @@ def test_bf16_rounds_to_nearest_even():
     assert list(got) == [1.0, 1.0, 1.0 + 2**-7, 1.0 + 2**-6, -2.5, 0.0]
 
 
-def test_backward_equals_central_differences(monkeypatch):
+@pytest.mark.parametrize("delta", [0.0, 0.7])
+def test_backward_equals_central_differences(monkeypatch, delta):
     monkeypatch.setattr(ref, "bf16", lambda a: np.asarray(a, dtype=np.float64))
     monkeypatch.setattr(ref, "FLOAT", np.float64)
     rng = np.random.default_rng(0)
@@ -26,11 +28,11 @@ def test_backward_equals_central_differences(monkeypatch):
 
     def loss_of(q):
         pred, _, _ = ref.forward(feat, [(w.astype(np.float64), b) for w, b in ref.unpack(q, shapes)])
-        return ref.loss_grad(pred.astype(np.float64), tgt, wts, heads, nt)[1]
+        return ref.loss_grad(pred.astype(np.float64), tgt, wts, heads, nt, delta)[1]
 
     layers = ref.unpack(p, shapes)
     pred, a, z = ref.forward(feat, layers)
-    dpred, _ = ref.loss_grad(pred.astype(np.float64), tgt, wts, heads, nt)
+    dpred, _ = ref.loss_grad(pred.astype(np.float64), tgt, wts, heads, nt, delta)
     grads = ref.backward(dpred, layers, a, z)
     flat = np.concatenate([np.concatenate([gw.ravel(), gb]) for gw, gb in grads])
     eps = 1e-6
