@@ -502,7 +502,8 @@ def run_uneven(args) -> None:
     """Uneven batching: 262,144 cells of the column grid, the night half dark, settled by four 300 s calls, then a
     quarter turned into cold starts (h 1e-10 s, x perturbed log-normally); a loop of --calls 300 s calls, each from
     the previous call's x and h. Reports the per-call latency (p50, p99) of the loop run call by call with the
-    autotuned persistent grid and with one CTA per cell, and cells/s of the loop captured in one CUDA graph."""
+    autotuned mapping (2 or 4 warps per cell) and persistent grid and with one CTA per cell, and cells/s of the loop
+    captured in one CUDA graph. --network picks the network (the configuration's is the 69-species one)."""
     import torch
 
     from maxichem_b200 import autotune, graph, synthetic
@@ -510,17 +511,19 @@ def run_uneven(args) -> None:
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    net = synthetic.network(NETWORK)
+    net = synthetic.network(args.network)
     B = min(args.cells, 262144)
     w = synthetic.workload(net, "uneven", B, seed=11)
     t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
-    solver = CudaSolver(net, dev, photo=True)
+    spin = CudaSolver(net, dev, photo=True)
     x, T, P, dt, h, J = t(w.x), t(w.T), t(w.P), t(w.dt), t(w.h), t(w.J)
     for _ in range(SPINUP_CALLS):
-        x, h, _, _ = solver(x, T, P, dt, h, J=J)
+        x, h, _, _ = spin(x, T, P, dt, h, J=J)
+    spin.close()
     xc, hc, cold = synthetic.cold_start(x.cpu().numpy(), h.cpu().numpy(), seed=12)
     x0, h0 = t(xc), t(hc)
-    tuned = autotune.tune_grid(solver, x0, T, P, dt, h0, J=J)
+    solver, tuned = autotune.tune(net, dev, x0, T, P, dt, h0, J=J)
+    tuned["best"] = tuned["grid"]
     stream = torch.cuda.current_stream(dev)
 
     def loop(grid: int) -> dict:
@@ -556,9 +559,10 @@ def run_uneven(args) -> None:
     done_all = bool(last["done"].bool().all())
     cl.close()
     line = {
-        "metric": "cells/s of a GCM call loop with uneven step counts (69-sp, 262,144 cells)", "unit": "cells/s",
+        "metric": f"cells/s of a GCM call loop with uneven step counts ({solver.ns}-sp, {B} cells)", "unit": "cells/s",
         "workload": "uneven", "cells": B, "calls": args.calls, "cold_cells": int(cold.sum()),
-        "autotune_ms": {str(k): v for k, v in tuned["ms"].items()}, "autotune_best_ctas_per_sm": tuned["best"],
+        "autotune_ms": {f"{k[0]} warps, {k[1]} ctas/sm": v for k, v in tuned["ms"].items()},
+        "autotune_best": {"warps_per_cell": tuned["warps"], "ctas_per_sm": tuned["grid"]},
         "persistent": persistent, "static_one_cta_per_cell": static,
         "graph": {"ms": graph_ms, "cells_per_s": B * args.calls / (graph_ms * 1e-3), "last_call_all_done": done_all},
         "data": "synthetic (seeded 69-species network, column grid, night half dark, quarter cold starts)",

@@ -224,10 +224,12 @@ int mx_jvp(mx_solver* s, const double* x, const double* T, const double* P, cons
  * Outputs as mx_call's, and gx0 [B][ns], gT, gP, gdt, gh0 [B], glm [B][nr], gJ [B][nj] (NULL when nj == 0) per cell,
  * and grc [nr][9], the rate table's nine Arrhenius columns, summed over the cells in a fixed order. A cell that still
  * fails (flag 2) has NaN cotangents and is left out of grc, as is a refused cell. Results do not depend on the batch
- * order or on the launch: no atomics enter the arithmetic. Allocates the adjoint's scratch at the first call and when
- * a call needs more: per CTA 14 nr + 4 cap (ns + 8) doubles, and per cell 3 nr doubles (the rate table's per-cell
- * cotangents, summed over the cells in a fixed order; 10.5 GB at 1,048,576 cells of 438 reactions). Calls run one at
- * a time.
+ * order or on the launch: no atomics enter the arithmetic (grc is summed over fixed chunks of 64 consecutive cells
+ * and then over the chunks in order, so it keeps its bits for a given batch). Allocates the adjoint's scratch at the
+ * first call and when a call needs more: per CTA 17 nr + 4 cap (ns + 8) doubles, per chunk of 64 cells 9 nr doubles
+ * (the chunk's partial sum of the rate table's cotangent: 0.5 GB at 1,048,576 cells of 438 reactions), and 3 nr
+ * doubles per cell the recovery redoes; one small host read of the count of those cells (a synchronisation of
+ * the stream). Calls run one at a time.
  */
 int mx_vjp(mx_solver* s, const double* x, const double* T, const double* P, const double* dt, const double* h_in,
            const double* J, const double* lm, const double* rc, int64_t B, double rtol, double atol, int32_t max_steps,

@@ -60,8 +60,12 @@ struct mx_derivatives {
   const uint64_t* st8 = nullptr;                  // S's columns (in the solver's buffers)
   double* vjp_scratch = nullptr;
   size_t vjp_scratch_doubles = 0;
-  double* vjp_gl = nullptr;
-  size_t vjp_gl_doubles = 0;
+  double* vjp_glc = nullptr;  // the rate table's chunk partial sums [nr][chunks][9]
+  size_t vjp_glc_doubles = 0;
+  double* vjp_glq = nullptr;  // recovered cells' rate-table cotangents [listed][nr][3]
+  size_t vjp_glq_doubles = 0;
+  int* vjp_ints = nullptr;    // chunk flags [chunks], the chunk queue [1], list slots [B]
+  size_t vjp_ints_count = 0;
 };
 
 namespace {
@@ -79,7 +83,9 @@ void mx_release_derivatives(mx_solver* s) {
   if (!d) return;
   if (d->jvp_scratch) cudaFree(d->jvp_scratch);
   if (d->vjp_scratch) cudaFree(d->vjp_scratch);
-  if (d->vjp_gl) cudaFree(d->vjp_gl);
+  if (d->vjp_glc) cudaFree(d->vjp_glc);
+  if (d->vjp_glq) cudaFree(d->vjp_glq);
+  if (d->vjp_ints) cudaFree(d->vjp_ints);
   delete d;
   s->deriv = nullptr;
 }
@@ -383,29 +389,56 @@ extern "C" int mx_vjp(mx_solver* s, const double* x, const double* T, const doub
   if (rcode) return rcode;
   const Net& n0 = s->net;
   const int stored = 2 * cap;
-  const long long slot = ((long long)14 * n0.nr + 2LL * stored * (n0.ns + REC_EXTRA) + 1) & ~1ll;
-  const int grid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)d->vjp_ctas * s->sms);
+  // per CTA: k_bar, c1, c2, the try states, the cell's rate-table cotangents (3 nr)
+  const long long slot = ((long long)17 * n0.nr + 2LL * stored * (n0.ns + REC_EXTRA) + 1) & ~1ll;
+  const int nchunks = (int)((std::max<int64_t>(B, 1) + ADJ_CHUNK - 1) / ADJ_CHUNK);
+  const int grid = (int)std::min<int64_t>(nchunks, (int64_t)d->vjp_ctas * s->sms);
   const int rgrid = (int)std::min<int64_t>(std::max<int64_t>(B, 1), (int64_t)d->vjp_recover_ctas * s->sms);
   rcode = grow_doubles(&d->vjp_scratch, &d->vjp_scratch_doubles, (size_t)std::max(grid, rgrid) * (size_t)slot,
                        "adjoint scratch", err, errlen);
   if (rcode) return rcode;
-  rcode = grow_doubles(&d->vjp_gl, &d->vjp_gl_doubles, (size_t)std::max<int64_t>(B, 1) * n0.nr * 3,
-                       "per-cell rate-table cotangents", err, errlen);
+  rcode = grow_doubles(&d->vjp_glc, &d->vjp_glc_doubles, (size_t)n0.nr * nchunks * 9,
+                       "the rate table's chunk sums", err, errlen);
   if (rcode) return rcode;
+  const size_t ints = (size_t)nchunks + 1 + (size_t)std::max<int64_t>(B, 1);
+  if (ints > d->vjp_ints_count) {
+    if (d->vjp_ints) cudaFree(d->vjp_ints);
+    d->vjp_ints = nullptr;
+    d->vjp_ints_count = 0;
+    if (cudaMalloc(&d->vjp_ints, ints * sizeof(int)) != cudaSuccess) {
+      set_error(err, errlen, "mx_vjp: the chunk flags and list slots of %lld cells", (long long)B);
+      return MX_ERR_CUDA;
+    }
+    d->vjp_ints_count = ints;
+  }
+  int* chunk_listed = d->vjp_ints;
+  int* chunk_queue = d->vjp_ints + nchunks;
+  int* pos = chunk_queue + 1;
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = cudaMemsetAsync(count, 0, MX_COUNT_SLOTS * sizeof(int32_t), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(chunk_queue, 0, sizeof(int), st);
   if (e == cudaSuccess && B > 0) {
     Net net = s->net;
     if (rc) net.rc = rc;  // the caller's rate table
     const CallArgs a{x, T, P, dt, h_in, J, (int)B, rtol, atol, max_steps, x_out, h_out, done, steps, flag, status,
                      count, s->list, nullptr};
-    const AdjArgs aa{lm, gx, gh, adapt, stored, gx0, gT, gP, gdt, gh0, glm, s->net.nj > 0 ? gJ : nullptr,
-                     d->vjp_gl, d->vjp_scratch, slot, d->sp_ptr, d->sp_ent, d->st8};
+    AdjArgs aa{lm, gx, gh, adapt, stored, gx0, gT, gP, gdt, gh0, glm, s->net.nj > 0 ? gJ : nullptr, d->vjp_glc,
+               nchunks, chunk_listed, chunk_queue, nullptr, pos, d->vjp_scratch, slot, d->sp_ptr, d->sp_ent, d->st8};
     d->vjp<<<grid, 32 * WARPS, d->vjp_smem, st>>>(net, a, aa, d->adj_layout);
-    d->vjp_recover<<<rgrid, 32 * WARPS, d->vjp_smem, st>>>(net, a, aa, d->adj_layout, MX_REC_STEPS * max_steps);
-    arrh_kernel<<<n0.nr, ARRH_THREADS, 0, st>>>(net, a, d->vjp_gl, grc);
-    e = cudaGetLastError();
-  } else if (e == cudaSuccess) {
+    // the recovered cells' cotangents get a slot each: size them from the count of listed cells (one small read)
+    int listed = 0;
+    e = cudaMemcpyAsync(&listed, count + MX_COUNT_RECOMPUTED, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) {
+      rcode = grow_doubles(&d->vjp_glq, &d->vjp_glq_doubles, (size_t)std::max(listed, 1) * n0.nr * 3,
+                           "the recovered cells' rate-table cotangents", err, errlen);
+      if (rcode) return rcode;
+      aa.gLq = d->vjp_glq;
+      d->vjp_recover<<<rgrid, 32 * WARPS, d->vjp_smem, st>>>(net, a, aa, d->adj_layout, MX_REC_STEPS * max_steps);
+      arrh_kernel<<<n0.nr, 32, 0, st>>>(net, a, aa, grc);
+      e = cudaGetLastError();
+    }
+  } else if (e == cudaSuccess && grc) {  // an empty batch: the rate table's cotangent is zero (if asked for)
     e = cudaMemsetAsync(grc, 0, (size_t)n0.nr * 9 * sizeof(double), st);
   }
   if (e == cudaSuccess) {

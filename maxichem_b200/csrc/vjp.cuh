@@ -10,7 +10,10 @@
 // sum_k b_k^T J_N K_k, whose Jacobian part comes reaction by reaction from second products of the concentrations.
 // Species sums gather each species' reaction slots from a table in a fixed order: no atomics enter the arithmetic,
 // so the same inputs give the same bits. The rate cotangents reduce to T, P, the log multipliers and J per cell, and
-// to the rate table's Arrhenius columns in a second kernel that sums over the cells in a fixed order.
+// to the rate table's Arrhenius columns: the forward kernel takes cells in fixed chunks of ADJ_CHUNK consecutive
+// cells from its queue and adds each passing cell's contribution to its chunk's partial sum in cell order; a cell the
+// recovery redoes leaves its contribution in a slot of its own; a last kernel adds the chunks and those slots in a
+// fixed order.
 #pragma once
 #include "jvp.cuh"
 
@@ -20,7 +23,13 @@ namespace mx {
 struct AdjArgs {
   const double *lm, *gx, *gh;
   int adapt, cap;  // cap: stored try states per cell (2 cap of checkpoints and of segment states)
-  double *gx0, *gT, *gP, *gdt, *gh0, *glm, *gJ, *gL;  // gL [B][nr][3]: per cell the cotangents of ln k0's terms, k_inf
+  double *gx0, *gT, *gP, *gdt, *gh0, *glm, *gJ;
+  double* gLc;        // [nr][nchunks][9]: per chunk the rate-table cotangent of its cells that passed the guard
+  int nchunks;
+  int* chunk_listed;  // [nchunks]: 1 when a cell of the chunk went to the recovery
+  int* chunk_queue;   // the forward kernel's chunk queue
+  double* gLq;        // [listed][nr][3]: a recovered cell's cotangents of ln k0's terms and ln k_inf, by list slot
+  int* pos;           // [B]: a listed cell's slot in the recovery's list
   double* scratch;
   long long slot;
   const int *sp_ptr, *sp_ent;  // species gather: species j's reaction slots sp_ent[sp_ptr[j] .. sp_ptr[j + 1]) = r*8 + m
@@ -55,13 +64,18 @@ __device__ __forceinline__ AdjCell adj_arrays(const AdjLayout& l, double* smem) 
   return a;
 }
 
-// per-CTA scratch: k_bar [2 nr], slot contributions c1 [nr][6], c2 [nr][6], try states [2][cap][ns + 8]
+// per-CTA scratch: k_bar [2 nr], slot contributions c1 [nr][6], c2 [nr][6], try states [2][cap][ns + 8], the cell's
+// cotangents of ln k0's terms and ln k_inf [nr][3]
 constexpr int REC_EXTRA = 8;  // h, t, pen, pha, prej, nok and two spare
+constexpr int ADJ_CHUNK = 64;  // cells per chunk of the rate table's partial sums
 __device__ __forceinline__ double* adj_kbar(const Net& net, double* sl) { return sl; }
 __device__ __forceinline__ double* adj_c1(const Net& net, double* sl) { return sl + 2 * net.nr; }
 __device__ __forceinline__ double* adj_c2(const Net& net, double* sl) { return sl + 8 * net.nr; }
 __device__ __forceinline__ double* adj_state(const Net& net, const AdjArgs& aa, double* sl, int bank, int i) {
   return sl + 14 * net.nr + ((size_t)bank * aa.cap + i) * (net.ns + REC_EXTRA);
+}
+__device__ __forceinline__ double* adj_gl(const Net& net, const AdjArgs& aa, double* sl) {
+  return sl + 14 * net.nr + (size_t)2 * aa.cap * (net.ns + REC_EXTRA);
 }
 
 // a block-wide sum in a fixed order: every thread's value, then thread 0 adds them in thread order; every thread
@@ -730,7 +744,7 @@ __device__ void rates_adjoint(const Net& net, const Cell& c, const AdjCell& b, c
     const double kf = c.kf[r], kr = c.kr[r];
     const double gf = kb[r] * kf, gr = kb[nr + r] * kr;  // cotangents of ln kf, ln kr
     if (aa.glm) aa.glm[(size_t)cell * nr + r] = gf + gr;
-    double* gl = aa.gL + ((size_t)cell * nr + r) * 3;
+    double* gl = adj_gl(net, aa, sl) + (size_t)r * 3;
     if (r >= net.nrt) {  // kf = J e^lm
       const int b = r - net.nrt;
       const double em = aa.lm ? exp(aa.lm[(size_t)cell * nr + r]) : 1.0;
@@ -850,7 +864,7 @@ __device__ void finish_cell(const Net& net, const Cell& c, const AdjCell& b, con
     for (int i = tid; i < ns; i += nt) aa.gx0[(size_t)cell * ns + __ldg(net.perm + i)] = q;
     for (int r = tid; r < net.nr; r += nt) {
       if (aa.glm) aa.glm[(size_t)cell * net.nr + r] = q;
-      double* gl = aa.gL + ((size_t)cell * net.nr + r) * 3;
+      double* gl = adj_gl(net, aa, sl) + (size_t)r * 3;
       gl[0] = gl[1] = gl[2] = q;
     }
     for (int j = tid; j < net.nj; j += nt) aa.gJ[(size_t)cell * net.nj + j] = q;
@@ -889,8 +903,35 @@ __device__ void finish_cell(const Net& net, const Cell& c, const AdjCell& b, con
 
 // ---- the kernels ----
 
+// A passing cell's rate-table cotangent (adj_gl) into its chunk's partial sum: per reaction (one thread) and
+// exponent e, the sum over the chunk's passing cells in cell order of g, g ln T and -g / T; the chunk's first
+// passing cell writes, the others add.
+__device__ __forceinline__ void add_to_chunk(const Net& net, const AdjArgs& aa, double* sl, int chunk, double Tc,
+                                             bool first, int tid, int nt) {
+  const double lT = log(Tc), iT = 1.0 / Tc;
+  const double* gl = adj_gl(net, aa, sl);
+  for (int r = tid; r < net.nr; r += nt) {
+    double* dst = aa.gLc + ((size_t)r * aa.nchunks + chunk) * 9;
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      const double g = gl[3 * r + e];
+      if (first) {
+        dst[3 * e] = g;
+        dst[3 * e + 1] = g * lT;
+        dst[3 * e + 2] = -g * iT;
+      } else {
+        dst[3 * e] += g;
+        dst[3 * e + 1] = fma(g, lT, dst[3 * e + 1]);
+        dst[3 * e + 2] = fma(-g, iT, dst[3 * e + 2]);
+      }
+    }
+  }
+}
+
 // The adjoint kernel: the call kernel's screening, rates, tries (each try's state stored), output and guard, then,
 // for a cell that passed the guard, the reverse pass and its cotangents. A listed cell is left to the recovery's.
+// Cells come in chunks of ADJ_CHUNK consecutive cells from the queue, each chunk's cells in order, so each chunk's
+// partial sum of the rate table's cotangent is formed by one CTA in a fixed order.
 template <int W, int R>
 __global__ void __launch_bounds__(32 * W, 3) vjp_kernel(const Net net, const CallArgs a, const AdjArgs aa,
                                                         const AdjLayout al) {
@@ -899,111 +940,130 @@ __global__ void __launch_bounds__(32 * W, 3) vjp_kernel(const Net net, const Cal
   const AdjCell b = adj_arrays(al, smem);
   const int tid = (int)threadIdx.x, nt = 32 * W, lane = tid & 31, warp = tid >> 5, ns = net.ns;
   double* sl = aa.scratch + (size_t)blockIdx.x * aa.slot;
-  int cell = (int)blockIdx.x;
-  while (cell < a.B) {
-    const double Tc = a.T[cell], dt = a.dt[cell], hin = a.h_in[cell], P = a.P[cell];
-    const double nd = P / (MX_KB * Tc);
-    const double* x0 = a.x + (size_t)cell * ns;
-    const double* Jc = a.J + (size_t)cell * net.nj;
-    const double* lmc = aa.lm ? aa.lm + (size_t)cell * net.nr : nullptr;
-    for (int i = tid; i < ns; i += nt) c.N[i] = x0[__ldg(net.perm + i)];
-    __syncthreads();
-    if (warp == 0) {  // screening, as the call kernel's
-      const double nan = __longlong_as_double(0x7ff8000000000000ll);
-      double p = 0.0, pm = 0.0;
-      for (int i = lane; i < ns; i += 32) {
-        const double xi = c.N[i];
-        p += xi >= 0.0 ? xi : nan;
-        pm = fmax(pm, xi);
-      }
-      for (int j = lane; j < net.nj; j += 32) {
-        const double q = Jc[j];
-        p += q >= 0.0 ? 0.0 * q : nan;
-      }
-      const double ps = warp_sum(p), mxv = warp_max(pm);
-      const bool forcing = isfinite(Tc) && isfinite(nd) && nd > 0.0 && isfinite(dt) && dt >= 0.0;
-      const bool fine = fabs(ps - 1.0) <= MX_X_SUM_TOL && mxv > 0.0 && forcing;
-      const int st =
-          Tc < MX_T_MIN ? MX_REFUSED_COLD : (Tc > MX_T_MAX ? MX_REFUSED_HOT : (fine ? 0 : MX_REFUSED_BAD_INPUT));
-      if (lane == 0) {
-        c.ints[0] = st;
-        a.status[cell] = st;
-        if (!isfinite(hin)) atomicAdd(a.count + MX_COUNT_NONFINITE_H, 1);
-      }
-    }
-    __syncthreads();
-    const int st = c.ints[0];
-    const bool lm_fine = multipliers_finite(net, lmc, tid);
-    if (st == 0) {
-      cell_rates(net, c, Tc, nd, Jc, tid, nt);
-      if (lmc) apply_multipliers(net, c, lmc, tid, nt);
-    }
-    const double h0 = isfinite(hin) ? hin : dt;
-    StepState s = {fmax(fmin(h0, dt), MX_H_MIN), 0.0, 0.0, 0.0, 0.0, false};
-    const StepState s0 = s;
-    int it = (dt > 0.0 && st == 0 && lm_fine) ? 0 : a.max_steps, n = 0;
-    while (it < a.max_steps && s.t < dt * MX_CALL_END) {
-      if (n < aa.cap) store_state(net, c, adj_state(net, aa, sl, 0, n), s, tid, nt);
-      double c0 = 0.0;
-      primal_try<W, R, false>(net, c, s, dt, nd, a.rtol, a.atol, nullptr, c0, tid);
-      primal_update(net, c, s, dt, tid, nt);
-      it++;
-      n++;
-    }
-    if (warp == 0) {
-      const double sum = lane_sum(c.N, ns, lane);
-      if (lane == 0) c.red[3] = sum;
-    }
-    __syncthreads();
-    const double sum = c.red[3];
-    for (int i = tid; i < ns; i += nt) c.Y[__ldg(net.perm + i)] = c.N[i] / sum;
-    const double *at = net.atoms, *xin = x0;
-    stage_guard_inputs(net, c, x0, tid, nt, &at, &xin);
-    __syncthreads();
-    if (warp == 0) {
-      const int done = (st == 0 && s.t >= dt * MX_CALL_END) ? 1 : 0;
-      const int g = st == 0 ? check_cell(net, xin, c.Y, done, s.nok, a.atol, lane, at, c.G) : 0;
-      if (lane == 0) {
-        a.h_out[cell] = s.h;
-        a.done[cell] = done;
-        a.steps[cell] = s.nok;
-        int r = 0;
-        if (st == MX_REFUSED_COLD)
-          atomicAdd(a.count + MX_COUNT_COLD, 1);
-        else if (st == MX_REFUSED_HOT)
-          atomicAdd(a.count + MX_COUNT_HOT, 1);
-        else if (st == MX_REFUSED_BAD_INPUT)
-          atomicAdd(a.count + MX_COUNT_BAD_INPUT, 1);
-        else {
-          if (g & GUARD_NONFINITE) atomicAdd(a.count + MX_COUNT_NONFINITE, 1);
-          if (g & GUARD_UNFINISHED) atomicAdd(a.count + MX_COUNT_UNFINISHED, 1);
-          if (g & GUARD_DRIFT) atomicAdd(a.count + MX_COUNT_DRIFT, 1);
-          if (g) {
-            r = 1;
-            a.list[atomicAdd(a.count + MX_COUNT_RECOMPUTED, 1)] = cell;
-          }
-        }
-        a.flag[cell] = r;
-        c.ints[2] = r;
-        c.ints[1] = (int)(gridDim.x + atomicAdd(a.count + MX_COUNT_QUEUE, 1));
-      }
-    }
-    __syncthreads();
-    double* xo = a.x_out + (size_t)cell * ns;
-    for (int i = tid; i < ns; i += nt) xo[i] = c.Y[i];
-    const int listed = c.ints[2];
-    if (!listed) {  // a listed cell's cotangents come from the recovery
-      double* kb = adj_kbar(net, sl);
-      for (int r = tid; r < 2 * net.nr; r += nt) kb[r] = 0.0;
-      StepBar sb = {aa.adapt && aa.gh ? aa.gh[cell] : 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int chunk = (int)blockIdx.x;
+  while (chunk < aa.nchunks) {
+    const int first_cell = chunk * ADJ_CHUNK, end_cell = min(a.B, first_cell + ADJ_CHUNK);
+    bool started = false, any_listed = false;
+    for (int cell = first_cell; cell < end_cell; cell++) {
+      const double Tc = a.T[cell], dt = a.dt[cell], hin = a.h_in[cell], P = a.P[cell];
+      const double nd = P / (MX_KB * Tc);
+      const double* x0 = a.x + (size_t)cell * ns;
+      const double* Jc = a.J + (size_t)cell * net.nj;
+      const double* lmc = aa.lm ? aa.lm + (size_t)cell * net.nr : nullptr;
+      for (int i = tid; i < ns; i += nt) c.N[i] = x0[__ldg(net.perm + i)];
       __syncthreads();
-      if (st == 0) {
-        x_adjoint(net, c, b, aa, cell, sum, tid, nt);
-        reverse_pass<W, R, false>(net, c, b, aa, sl, s0, n, dt, nd, nullptr, a.rtol, a.atol, sb, tid);
+      if (warp == 0) {  // screening, as the call kernel's
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        double p = 0.0, pm = 0.0;
+        for (int i = lane; i < ns; i += 32) {
+          const double xi = c.N[i];
+          p += xi >= 0.0 ? xi : nan;
+          pm = fmax(pm, xi);
+        }
+        for (int j = lane; j < net.nj; j += 32) {
+          const double q = Jc[j];
+          p += q >= 0.0 ? 0.0 * q : nan;
+        }
+        const double ps = warp_sum(p), mxv = warp_max(pm);
+        const bool forcing = isfinite(Tc) && isfinite(nd) && nd > 0.0 && isfinite(dt) && dt >= 0.0;
+        const bool fine = fabs(ps - 1.0) <= MX_X_SUM_TOL && mxv > 0.0 && forcing;
+        const int st =
+            Tc < MX_T_MIN ? MX_REFUSED_COLD : (Tc > MX_T_MAX ? MX_REFUSED_HOT : (fine ? 0 : MX_REFUSED_BAD_INPUT));
+        if (lane == 0) {
+          c.ints[0] = st;
+          a.status[cell] = st;
+          if (!isfinite(hin)) atomicAdd(a.count + MX_COUNT_NONFINITE_H, 1);
+        }
       }
-      finish_cell(net, c, b, aa, sl, cell, Tc, P, nd, hin, dt, 0, sb, st != 0, c.v, b.Nn, tid, nt);
+      __syncthreads();
+      const int st = c.ints[0];
+      const bool lm_fine = multipliers_finite(net, lmc, tid);
+      if (st == 0) {
+        cell_rates(net, c, Tc, nd, Jc, tid, nt);
+        if (lmc) apply_multipliers(net, c, lmc, tid, nt);
+      }
+      const double h0 = isfinite(hin) ? hin : dt;
+      StepState s = {fmax(fmin(h0, dt), MX_H_MIN), 0.0, 0.0, 0.0, 0.0, false};
+      const StepState s0 = s;
+      int it = (dt > 0.0 && st == 0 && lm_fine) ? 0 : a.max_steps, n = 0;
+      while (it < a.max_steps && s.t < dt * MX_CALL_END) {
+        if (n < aa.cap) store_state(net, c, adj_state(net, aa, sl, 0, n), s, tid, nt);
+        double c0 = 0.0;
+        primal_try<W, R, false>(net, c, s, dt, nd, a.rtol, a.atol, nullptr, c0, tid);
+        primal_update(net, c, s, dt, tid, nt);
+        it++;
+        n++;
+      }
+      if (warp == 0) {
+        const double sum = lane_sum(c.N, ns, lane);
+        if (lane == 0) c.red[3] = sum;
+      }
+      __syncthreads();
+      const double sum = c.red[3];
+      for (int i = tid; i < ns; i += nt) c.Y[__ldg(net.perm + i)] = c.N[i] / sum;
+      const double *at = net.atoms, *xin = x0;
+      stage_guard_inputs(net, c, x0, tid, nt, &at, &xin);
+      __syncthreads();
+      if (warp == 0) {
+        const int done = (st == 0 && s.t >= dt * MX_CALL_END) ? 1 : 0;
+        const int g = st == 0 ? check_cell(net, xin, c.Y, done, s.nok, a.atol, lane, at, c.G) : 0;
+        if (lane == 0) {
+          a.h_out[cell] = s.h;
+          a.done[cell] = done;
+          a.steps[cell] = s.nok;
+          int r = 0;
+          if (st == MX_REFUSED_COLD)
+            atomicAdd(a.count + MX_COUNT_COLD, 1);
+          else if (st == MX_REFUSED_HOT)
+            atomicAdd(a.count + MX_COUNT_HOT, 1);
+          else if (st == MX_REFUSED_BAD_INPUT)
+            atomicAdd(a.count + MX_COUNT_BAD_INPUT, 1);
+          else {
+            if (g & GUARD_NONFINITE) atomicAdd(a.count + MX_COUNT_NONFINITE, 1);
+            if (g & GUARD_UNFINISHED) atomicAdd(a.count + MX_COUNT_UNFINISHED, 1);
+            if (g & GUARD_DRIFT) atomicAdd(a.count + MX_COUNT_DRIFT, 1);
+            if (g) {
+              r = 1;
+              a.list[atomicAdd(a.count + MX_COUNT_RECOMPUTED, 1)] = cell;
+            }
+          }
+          a.flag[cell] = r;
+          c.ints[2] = r;
+        }
+      }
+      __syncthreads();
+      double* xo = a.x_out + (size_t)cell * ns;
+      for (int i = tid; i < ns; i += nt) xo[i] = c.Y[i];
+      const int listed = c.ints[2];
+      if (!listed) {  // a listed cell's cotangents come from the recovery
+        double* kb = adj_kbar(net, sl);
+        for (int r = tid; r < 2 * net.nr; r += nt) kb[r] = 0.0;
+        StepBar sb = {aa.adapt && aa.gh ? aa.gh[cell] : 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        __syncthreads();
+        if (st == 0) {
+          x_adjoint(net, c, b, aa, cell, sum, tid, nt);
+          reverse_pass<W, R, false>(net, c, b, aa, sl, s0, n, dt, nd, nullptr, a.rtol, a.atol, sb, tid);
+        }
+        finish_cell(net, c, b, aa, sl, cell, Tc, P, nd, hin, dt, 0, sb, st != 0, c.v, b.Nn, tid, nt);
+        if (st == 0) {  // a refused cell stays out of the rate table's sum
+          add_to_chunk(net, aa, sl, chunk, Tc, !started, tid, nt);
+          started = true;
+        }
+      } else {
+        any_listed = true;
+      }
+      __syncthreads();
     }
-    cell = c.ints[1];
+    if (!started)  // no passing cell: the chunk's partial sum is zero
+      for (int r = tid; r < net.nr; r += nt)
+        for (int k = 0; k < 9; k++) aa.gLc[((size_t)r * aa.nchunks + chunk) * 9 + k] = 0.0;
+    if (tid == 0) {
+      aa.chunk_listed[chunk] = any_listed ? 1 : 0;
+      atomicAdd(a.count + MX_COUNT_QUEUE, end_cell - first_cell);
+      c.ints[1] = (int)(gridDim.x + atomicAdd(aa.chunk_queue, 1));
+    }
+    __syncthreads();
+    chunk = c.ints[1];
     __syncthreads();
   }
 }
@@ -1090,6 +1150,11 @@ __global__ void __launch_bounds__(32 * W, 3) vjp_recover_kernel(const Net net, c
           reverse_pass<W, R, true>(net, c, b, aa, sl, s0, n, dt, nd, pr, a.rtol, a.atol, sb, tid);
         }
         finish_cell(net, c, b, aa, sl, cell, Tc, P, nd, hin, dt, k, sb, failed, c.v, b.Nn, tid, nt);
+        // the cell's rate-table cotangent into its list slot, for the fixed-order sum
+        const double* gl = adj_gl(net, aa, sl);
+        for (int e = tid; e < 3 * net.nr; e += nt) aa.gLq[(size_t)q * 3 * net.nr + e] = gl[e];
+        if (tid == 0) aa.pos[cell] = q;
+        __syncthreads();
         q = nq;
         break;
       }
@@ -1097,38 +1162,28 @@ __global__ void __launch_bounds__(32 * W, 3) vjp_recover_kernel(const Net net, c
   }
 }
 
-// The rate table's cotangent: per reaction (one block), the sum over the cells in a fixed order of each cell's
-// cotangents of the three Arrhenius exponents times (1, ln T, -1 / T); cells that still fail (flag 2) or were
-// refused are left out. Photolysis rows are 0.
-constexpr int ARRH_THREADS = 256;
-__global__ void __launch_bounds__(ARRH_THREADS) arrh_kernel(const Net net, const CallArgs a, const double* gL,
-                                                            double* grc) {
-  __shared__ double part[ARRH_THREADS][9];
-  const int r = (int)blockIdx.x, tid = (int)threadIdx.x;
-  double acc[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+// The rate table's cotangent: per reaction (one block of 9 threads, one per column), the chunks' partial sums in
+// chunk order, each chunk followed by its recovered cells in cell order (their list slots' cotangents times 1, ln T,
+// -1 / T); cells that still fail (flag 2) or were refused are left out. Photolysis rows are 0. A fixed order: the
+// same inputs give the same bits, whatever the queues did.
+__global__ void arrh_kernel(const Net net, const CallArgs a, const AdjArgs aa, double* grc) {
+  const int r = (int)blockIdx.x, j = (int)threadIdx.x;
+  if (j >= 9) return;
+  double acc = 0.0;
   if (r < net.nrt) {
-    for (int cell = tid; cell < a.B; cell += ARRH_THREADS) {
-      if (a.flag[cell] == 2 || a.status[cell] != 0) continue;
-      const double T = a.T[cell], lT = log(T), iT = 1.0 / T;
-      const double* g = gL + ((size_t)cell * net.nr + r) * 3;
-#pragma unroll
-      for (int e = 0; e < 3; e++) {
-        acc[3 * e] += g[e];
-        acc[3 * e + 1] = fma(g[e], lT, acc[3 * e + 1]);
-        acc[3 * e + 2] = fma(-g[e], iT, acc[3 * e + 2]);
+    const int e = j / 3, kind = j % 3;
+    for (int k = 0; k < aa.nchunks; k++) {
+      acc += aa.gLc[((size_t)r * aa.nchunks + k) * 9 + j];
+      if (!aa.chunk_listed[k]) continue;
+      const int c1 = min(a.B, (k + 1) * ADJ_CHUNK);
+      for (int cell = k * ADJ_CHUNK; cell < c1; cell++) {
+        if (a.flag[cell] != 1) continue;  // passed (in the chunk's sum), still failed or refused
+        const double g = aa.gLq[((size_t)aa.pos[cell] * net.nr + r) * 3 + e], Tc = a.T[cell];
+        acc = kind == 0 ? acc + g : (kind == 1 ? fma(g, log(Tc), acc) : fma(-g, 1.0 / Tc, acc));
       }
     }
   }
-#pragma unroll
-  for (int k = 0; k < 9; k++) part[tid][k] = acc[k];
-  __syncthreads();
-  for (int w = ARRH_THREADS / 2; w > 0; w >>= 1) {
-    if (tid < w)
-#pragma unroll
-      for (int k = 0; k < 9; k++) part[tid][k] += part[tid + w][k];
-    __syncthreads();
-  }
-  if (tid < 9) grc[(size_t)r * 9 + tid] = part[0][tid];
+  grc[(size_t)r * 9 + j] = acc;
 }
 
 }  // namespace mx

@@ -75,9 +75,11 @@ def test_gradients_match_the_cpu_reference_layer_by_layer(small, gpu, delta):
         ew = np.linalg.norm(gw - rw) / np.linalg.norm(rw)
         eb = np.linalg.norm(gb - rb) / max(np.linalg.norm(rb), 1e-30)
         assert ew <= GRAD_RTOL and eb <= GRAD_RTOL, (l, ew, eb)
-    # the forward pass of the library equals the reference's (same BF16 operands, FP32 sums in another order)
+    # the forward pass of the library equals the reference's: the same BF16 operands, FP32 sums in another order, so
+    # an activation now and then rounds to the neighbouring BF16 value (2^-8 relative) and the five layers carry it on
     got = sur.forward(feat).cpu().numpy()
-    assert np.abs(got - pred).max() <= 1e-3 * np.abs(pred).max()
+    assert np.abs(got - pred).max() <= 5e-3 * np.abs(pred).max()
+    assert np.linalg.norm(got - pred) <= 1e-3 * np.linalg.norm(pred)
     sur.close()
 
 
