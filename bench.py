@@ -8,6 +8,8 @@ step is then the fifth 300 s call (x, T, P, dt, h, J resident in HBM), repeated 
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--cells B] [--impl ours|reference]
   python bench.py --derivative jvp|vjp [--directions D] [--frozen] [--cells B]   (the derivative calls)
+  python bench.py --workload uneven [--network N] [--calls C]                    (a call loop with cold starts)
+  python bench.py --workload mlp [--cells B]           (the surrogate network's forward and training step alone)
 
 --impl reference times the CPU implementation of the same solve (the oracle, a C restatement of the reference's
 kernels, on all host threads) on a bounded sample of the same cells; rank 0 alone runs it.
@@ -51,8 +53,9 @@ def parse() -> argparse.Namespace:
     p.add_argument("--cpu-sample", type=int, default=262144, help="cells of the CPU baseline sample")
     p.add_argument("--ref-sample", type=int, default=32768,
                    help="cells of the reference arm's sample (its four spin-up calls run on the CPU too)")
-    p.add_argument("--workload", choices=("column", "uneven"), default="column",
-                   help="uneven: 262,144 cells, half at night, a quarter cold starts, a loop of --calls calls")
+    p.add_argument("--workload", choices=("column", "uneven", "mlp"), default="column",
+                   help="uneven: 262,144 cells, half at night, a quarter cold starts, a loop of --calls calls; "
+                        "mlp: the surrogate network's forward pass and training step on --cells rows")
     p.add_argument("--calls", type=int, default=100, help="calls of the uneven workload's loop")
     p.add_argument("--network", choices=("cho41", "chno69", "sncho91"), default=NETWORK,
                    help="the synthetic network (the metric is quoted on chno69)")
@@ -196,6 +199,9 @@ def main() -> None:
     launch_ranks(args)
     if args.workload == "uneven":
         run_uneven(args)
+        return
+    if args.workload == "mlp":
+        run_mlp(args)
         return
     if args.derivative:
         run_derivative(args)
@@ -426,6 +432,59 @@ def mlp_roofline(sur, x, T, P, dt, h, J, stream) -> dict:
     return {"bound": "tensor", "kernel": "gemm_kernel (the network's 5 layers)", "achieved": flop / ms / 1e9,
             "peak": peak, "unit": "TFLOP/s", "frac": flop / ms / 1e9 / peak, "ms_per_forward": ms,
             "flops_per_forward": flop, "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained"}  # fmt: skip
+
+
+def run_mlp(args) -> None:
+    """The surrogate network alone (69-species network's shapes: 4 x 512 SiLU layers, 4 heads, BF16 on the tcgen05
+    GEMM): rows/s of its forward pass and of one training step (forward, Huber loss, backward, Adam) on --cells rows of
+    seeded standard-normal features, weights at their seeded initial values. A step is one forward pass (K of them
+    between CUDA events after W warm-up ones); the forward's activations (--cells x 512 x 2 bytes per layer) exceed L2
+    from 131,072 rows up. The roofline is the GEMMs' FLOPs over the forward's time against the measured BF16 peak
+    (burst: the forward's launches are timed back to back for well under a second)."""
+    import torch
+
+    from maxichem_b200 import surrogate as sg
+    from maxichem_b200 import synthetic
+    from maxichem_b200.solver import CudaSolver
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    net = synthetic.network(args.network)
+    with CudaSolver(net, dev, photo=True) as solver:
+        ns, nj, atoms = solver.ns, solver.nj, solver.tab.atoms
+    rows = max(64, args.cells // 64 * 64)
+    sur = sg.Surrogate(ns, nj, atoms, dev, seed=1)
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    feat = torch.randn(rows, sur.kin, device=dev, generator=g).to(torch.bfloat16)
+    tgt = torch.randn(rows, sur.nt, device=dev, generator=g)
+    wts = torch.ones(rows, sur.heads, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    clock = Clocks(0)
+    with clock:
+        ms_fwd, _ = timed_steps(lambda: sur.forward(feat), args.steps, args.warmup, stream)
+        ms_train, _ = timed_steps(lambda: sur.train_step(feat, tgt, wts, 1e-4, delta=1.0), args.steps, args.warmup,
+                                  stream)  # fmt: skip
+    sur.check()
+    flop = 2.0 * rows * sum(r * c for r, c in sur.shapes)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("bf16_tflops", 1590.0)
+    achieved = flop / ms_fwd / 1e9
+    line = {"metric": f"rows/s of the surrogate's forward pass ({ns}-sp network's shapes, {rows} rows)",
+            "value": rows / ms_fwd * 1e3, "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_fwd, "higher_is_better": True, "dtype": "bf16", "data": "synthetic (seeded features)",
+            "config": {"workload": f"surrogate forward, {sur.kin} -> {sur.layers} x {sur.hidden} SiLU -> "
+                                   f"{sur.heads} x {sur.nt} heads (padded to {sur.kout})", "rows": rows},
+            "gpu_launches": (sur.layers + 1) * args.steps,
+            "roofline": {"bound": "tensor", "kernel": "gemm_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1590"},
+            "train_step": {"ms": ms_train, "rows_per_s": rows / ms_train * 1e3,
+                           "gemm_tflops": 3 * flop / ms_train / 1e9,
+                           "note": "forward, loss, backward (6 more GEMMs, transposes, column sums), Adam"},
+            "clocks": clock.summary()}  # fmt: skip
+    sur.close()
+    print(json.dumps(line), flush=True)
 
 
 def run_derivative(args) -> None:

@@ -386,7 +386,8 @@ int mx_sur_destroy(mx_surrogate* s);
 /* The surrogate's GEMM alone (a building block, exported for tests): C[M, N] = A[M, K] B[N, K]^T, A and B device BF16
  * row-major with leading dimensions lda, ldb (K and N multiples of 64). mode 0: out FP32 = C; 1: out FP32 = C + bias;
  * 2: z = C + bias (FP32 [M][ldz] when z is not null), out BF16 = silu(z); 3: out BF16 = C * silu'(z), z read.
- * *err_flag (device int32) is set when a wait gave up. Asynchronous on stream. */
+ * Every pointer (A, B, out, bias, z) and row pitch in bytes must be a multiple of 16, or MX_ERR_ARGUMENT is returned
+ * with nothing launched. *err_flag (device int32) is set when a wait gave up. Asynchronous on stream. */
 int mx_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int64_t M, int32_t N, int32_t K,
                  int32_t mode, const float* bias, float* z, int32_t ldz, void* out, int32_t ldo, int32_t* err_flag,
                  void* stream);

@@ -53,15 +53,33 @@ bool tensor_map(CUtensorMap* m, const void* p, uint64_t rows, uint64_t cols, uin
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// A tensor map for the epilogue's 32-row x 32-column pieces of an output (or of z) [rows][ld]: BF16 with the 64-byte
+// swizzle or FP32 with the 128-byte swizzle, the layouts the epilogue writes its staging in. False when the pointer or
+// the row pitch is not a multiple of 16 bytes or the encoding fails (the epilogue then stores directly, 16 bytes at a
+// time, which asks for the same alignment: the launcher refuses anything less).
+bool piece_map(CUtensorMap* m, const void* p, uint64_t rows, uint64_t cols, uint64_t ld, bool f32) {
+  const uint64_t es = f32 ? 4 : 2;
+  if (((uintptr_t)p & 15) || (ld * es) % 16) return false;
+  const cuuint64_t dims[2] = {cols, rows};
+  const cuuint64_t strides[1] = {ld * es};
+  const cuuint32_t box[2] = {(cuuint32_t)EPI_COLS, 32};
+  const cuuint32_t step[2] = {1, 1};
+  return g_encode(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                  const_cast<void*>(p), dims, strides, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  f32 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int g_sms = 0;
 
-template <int BN, int STAGES>
-cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int N, int K, const Epi& ep, int* err,
-                        cudaStream_t st) {
+template <int BN, int STAGES, int EPI>
+cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& to, const CUtensorMap& tz,
+                        int64_t M, int N, int K, const Epi& ep, int* err, cudaStream_t st) {
   static bool configured = false;  // per instance: the opt-in shared memory
   constexpr int smem = gemm_smem_bytes<BN, STAGES>();
+  static_assert(smem <= 232448, "more shared memory than a CTA of sm_100a may opt into");
   if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute((const void*)gemm_kernel<BN, STAGES>,
+    const cudaError_t e = cudaFuncSetAttribute((const void*)gemm_kernel<BN, STAGES, EPI>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     configured = true;
@@ -73,29 +91,54 @@ cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M,
   }
   const long long tiles = ((M + BM - 1) / BM) * (long long)(N / BN);
   const int grid = (int)std::min<long long>(tiles, std::max(g_sms, 1));  // persistent: one CTA per SM
-  gemm_kernel<BN, STAGES><<<grid, 192, smem, st>>>(ta, tb, (int)M, N, K, ep, err);
+  gemm_kernel<BN, STAGES, EPI><<<grid, THREADS, smem, st>>>(ta, tb, to, tz, (int)M, N, K, ep, err);
   return cudaGetLastError();
+}
+
+// the kernel for a column tile width and an epilogue
+template <int BN, int STAGES>
+cudaError_t launch_epi(int epi, const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& to,
+                       const CUtensorMap& tz, int64_t M, int N, int K, const Epi& ep, int* err, cudaStream_t st) {
+  switch (epi) {
+    case V_STORE: return launch_tile<BN, STAGES, V_STORE>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_BIAS: return launch_tile<BN, STAGES, V_BIAS>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_SILU: return launch_tile<BN, STAGES, V_SILU>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_SILU_Z: return launch_tile<BN, STAGES, V_SILU_Z>(ta, tb, to, tz, M, N, K, ep, err, st);
+    default: return launch_tile<BN, STAGES, V_DSILU>(ta, tb, to, tz, M, N, K, ep, err, st);
+  }
 }
 
 }  // namespace
 
 // C[M, N] = A[M, K] B[N, K]^T with the epilogue ep (gemm.cuh). Returns MX_ERR_ARGUMENT for shapes the kernel does not
-// take: K a multiple of 64, N of 64, leading dimensions multiples of 8 elements, 16-byte aligned pointers.
+// take: K a multiple of 64, N of 64, 16-byte aligned pointers (A, B, out, bias, z) and row pitches (lda, ldb, ldo,
+// ldz in bytes).
 int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, int N, int K, const Epi& ep, int* err,
                    cudaStream_t st) {
+  const bool f32_out = ep.mode == STORE || ep.mode == BIAS;
+  const bool has_bias = ep.mode == BIAS || ep.mode == BIAS_SILU, uses_z = (ep.mode == BIAS_SILU && ep.z) ||
+                                                                          ep.mode == DSILU;
   if (M < 1 || M > 0x7fffffff || N < 64 || N % 64 || K < 64 || K % 64 || lda < K || ldb < K || lda % 8 || ldb % 8 ||
-      ((uintptr_t)A & 15) || ((uintptr_t)B & 15) || !err || !ep.out || ep.ldo < N ||
-      ((ep.mode == BIAS || ep.mode == BIAS_SILU) && !ep.bias) || (ep.mode == DSILU && !ep.z))
+      ((uintptr_t)A & 15) || ((uintptr_t)B & 15) || !err || !ep.out || ((uintptr_t)ep.out & 15) || ep.ldo < N ||
+      ep.ldo % (f32_out ? 4 : 8) || (has_bias && (!ep.bias || ((uintptr_t)ep.bias & 15))) ||
+      (uses_z && (!ep.z || ((uintptr_t)ep.z & 15) || ep.ldz < N || ep.ldz % 4)))
     return MX_ERR_ARGUMENT;
   if (encoder() != cudaSuccess) return MX_ERR_CUDA;
   const int bn = N % 256 == 0 ? 256 : (N % 128 == 0 ? 128 : 64);  // the widest column tile that divides N
-  CUtensorMap ta, tb;
+  CUtensorMap ta, tb, to, tz;
   if (!tensor_map(&ta, A, (uint64_t)M, (uint64_t)K, (uint64_t)lda, BM) ||
       !tensor_map(&tb, B, (uint64_t)N, (uint64_t)K, (uint64_t)ldb, (uint32_t)bn))
     return MX_ERR_ARGUMENT;
-  const cudaError_t e = bn == 256   ? launch_tile<256, 4>(ta, tb, M, N, K, ep, err, st)
-                        : bn == 128 ? launch_tile<128, 6>(ta, tb, M, N, K, ep, err, st)
-                                    : launch_tile<64, 8>(ta, tb, M, N, K, ep, err, st);
+  // the epilogue's outputs go through TMA stores when their maps can be made, else through plain stores
+  Epi e2 = ep;
+  memset(&to, 0, sizeof(to));
+  memset(&tz, 0, sizeof(tz));
+  e2.tma = piece_map(&to, ep.out, (uint64_t)M, (uint64_t)N, (uint64_t)ep.ldo, f32_out) &&
+           (!uses_z || piece_map(&tz, ep.z, (uint64_t)M, (uint64_t)N, (uint64_t)ep.ldz, true));
+  const int epi = variant_of(ep.mode, ep.mode == BIAS_SILU && ep.z != nullptr);
+  const cudaError_t e = bn == 256   ? launch_epi<256, 3>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
+                        : bn == 128 ? launch_epi<128, 5>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
+                                    : launch_epi<64, 7>(epi, ta, tb, to, tz, M, N, K, e2, err, st);
   return e == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
@@ -103,7 +146,7 @@ extern "C" int mx_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t l
                             int32_t mode, const float* bias, float* z, int32_t ldz, void* out, int32_t ldo,
                             int32_t* err_flag, void* stream) {
   if (mode < STORE || mode > DSILU) return MX_ERR_ARGUMENT;
-  Epi ep{mode, bias, z, ldz, out, ldo};
+  Epi ep{mode, bias, z, ldz, out, ldo, 0};
   return mx_gemm_launch(A, lda, B, ldb, M, N, K, ep, err_flag, (cudaStream_t)stream);
 }
 

@@ -69,3 +69,25 @@ def test_shapes_the_kernel_does_not_take_are_refused(gpu):
                                     out.data_ptr(), 64, flag.data_ptr(), None)  # fmt: skip
     assert rc == 1  # K must be a multiple of 64
     assert np.isfinite(out.cpu().numpy()).all()
+
+
+def test_unaligned_outputs_bias_or_z_are_refused(gpu):
+    """Outputs, biases and z go through 16-byte stores and loads (TMA or plain): a pointer or a row pitch that is not a
+    multiple of 16 bytes is refused before anything is launched, and the buffers stay as they were."""
+    M, N, K = 128, 64, 64
+    A = torch.zeros(M, K, dtype=torch.bfloat16, device=gpu)
+    B = torch.zeros(N, K, dtype=torch.bfloat16, device=gpu)
+    bias = torch.zeros(N + 4, device=gpu)
+    out = torch.full((M * (N + 4),), 7.0, device=gpu)
+    z = torch.full((M * (N + 4),), 7.0, device=gpu)
+    flag = torch.zeros(1, dtype=torch.int32, device=gpu)
+    lib = abi.library()
+    p = lambda *a: lib.mx_gemm_bf16(A.data_ptr(), K, B.data_ptr(), K, M, N, K, *a, flag.data_ptr(), None)
+    assert p(STORE, None, None, 0, out.data_ptr() + 4, N) == 1             # output 4 bytes off
+    assert p(STORE, None, None, 0, out.data_ptr(), N + 1) == 1             # FP32 pitch of 260 bytes
+    assert p(BIAS, bias.data_ptr() + 4, None, 0, out.data_ptr(), N) == 1   # bias 4 bytes off
+    assert p(BIAS_SILU, bias.data_ptr(), None, 0, out.data_ptr(), N + 4) == 1   # BF16 pitch of 136 bytes
+    assert p(BIAS_SILU, bias.data_ptr(), z.data_ptr(), N + 1, out.data_ptr(), N + 8) == 1  # z pitch
+    assert p(DSILU, None, z.data_ptr() + 8, N, out.data_ptr(), N) == 1     # z 8 bytes off
+    torch.cuda.synchronize(gpu)
+    assert bool((out == 7.0).all()) and bool((z == 7.0).all())
