@@ -85,6 +85,26 @@ def passed(rep: dict) -> bool:
     )
 
 
+STRICT_SHARE = 0.999  # the configuration-grid samples: share of cells within RTOL
+STRICT_FLIPS = 1e-3  # and of cells whose accepted steps differ
+
+
+def passed_strict(rep: dict) -> bool:
+    """The bar of a settled call on a sample of a configuration's grid, closer to a bitwise one: statuses, done
+    flags, guard flags and counts identical with no rounding flip excused, at least STRICT_SHARE of the cells within
+    RTOL on every species above FLOOR, none beyond WORST_RTOL, element shares to SHARE_TOL."""
+    return (
+        rep["status_equal"]
+        and rep["done_equal"]
+        and rep["flag_equal"]
+        and rep["counts_gpu"] == rep["counts_ref"]
+        and rep["share_within_rtol"] >= STRICT_SHARE
+        and rep["worst_rel"] <= WORST_RTOL
+        and rep["flips"] <= STRICT_FLIPS * rep["cells"]
+        and rep["share_rel"] <= SHARE_TOL
+    )
+
+
 def passed_calibrated(rep: dict, floor: dict) -> bool:
     """The bar of a call whose own rounding sensitivity exceeds RTOL (a cold start, or a long dark call): the GPU
     may differ from the oracle by no more than the oracle differs from itself when T moves by one ulp (floor), up to

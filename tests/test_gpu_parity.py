@@ -108,3 +108,4 @@ def test_a_4096_cell_sample_of_the_configuration_grid(gpu, networks, name, dt):
         assert parity.passed_calibrated(rep, floor), (k, rep)
     for rep, _ in reports[1:]:
         assert parity.passed(rep), rep
+        assert parity.passed_strict(rep), rep
