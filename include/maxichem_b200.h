@@ -406,6 +406,13 @@ const char* mx_version(void);
 int mx_warps_per_cell(void);
 int mx_warps_supported(int32_t warps);
 
+/* Cells of the network n that fit one SM of device by shared memory (one cell per CTA, the CTA's reserved shared
+ * memory included), or -MX_ERR_NETWORK / -MX_ERR_CUDA. Allocates nothing and needs no solver: a caller chooses the
+ * warps per cell with it before building the tables (maxichem_b200/solver.py takes 2 warps when at least 6 cells fit,
+ * so that the 2-warp kernels, 8 CTAs per SM by registers, hold at least half again as many cells as the 4-warp ones).
+ * n's stream fields are not read. No counterpart in the reference (its choice: maxichem/_constants.py:67-72). */
+int mx_cells_per_sm(const mx_network* n, int32_t device);
+
 #ifdef __cplusplus
 }
 #endif

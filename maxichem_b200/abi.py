@@ -181,6 +181,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "mx_version": (ctypes.c_char_p, []),
     "mx_warps_per_cell": (ctypes.c_int, []),
     "mx_warps_supported": (ctypes.c_int, [ctypes.c_int32]),
+    "mx_cells_per_sm": (ctypes.c_int, [_P, ctypes.c_int32]),
 }
 
 _lib: ctypes.CDLL | None = None

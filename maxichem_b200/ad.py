@@ -77,7 +77,7 @@ class ADSolver(CudaSolver):
             raise ValueError(f"cap: an integer expected, got {cap!r}") from None
         if cap < 1:
             raise ValueError(f"cap: at least 1 stored attempt expected, got {cap}")
-        super().__init__(net, device, drift=drift, photo=photo)
+        super().__init__(net, device, drift=drift, photo=photo, warps=4)  # the derivative kernels take 4
         self.cap = cap
         self._rc0 = torch.as_tensor(self.tab.rc, dtype=torch.float64).to(self.dev)
 

@@ -548,6 +548,44 @@ bool pick_kernels(int ns, mx_solver* s) {
 
 namespace {
 
+// The shared-memory layout of one cell (doubles): A [ns][ld], kf kr, v (or G/RT), n, N Y F U K1-K4 dinv, red, ints,
+// the S.v pieces' partial sums, and the guard's scratch; sets net's offsets and net.doubles.
+void cell_layout(const mx_network* n, Net& net) {
+  const int ns = n->ns, nr = n->nr;
+  net.ld = ns | 1;  // odd: a column of A is read without bank conflicts
+  int off = 0;
+  auto take = [&](int doubles) {
+    const int o = off;
+    off += (doubles + 1) & ~1;
+    return o;
+  };
+  net.oA = take(ns * net.ld);
+  net.a_doubles = ns * net.ld;
+  net.oK = take(2 * nr + 2);
+  net.oV = take(std::max(nr + 1, ns + 1));
+  net.on = take(ns + 1);
+  net.oN = take(ns);
+  net.oY = take(ns);
+  net.oF = take(ns);
+  net.oU = take(ns);
+  net.oK1 = take(ns);
+  net.oK2 = take(ns);
+  net.oK3 = take(ns);
+  net.oK4 = take(ns);
+  net.oD = take(ns);
+  net.oRed = take(8);
+  net.oInts = take((ns + 8) / 2 + 1);
+  net.oPart = take(n->n_pieces);
+  {  // the guard's scratch: in the matrix's space past the staged atoms and input row when it fits there
+    const int staged = (ns * n->nel + ns + 1) & ~1;
+    if (staged + guard_scratch(ns) <= ns * net.ld)
+      net.oG = net.oA + staged;
+    else
+      net.oG = take(guard_scratch(ns));
+  }
+  net.doubles = off;
+}
+
 void release(mx_solver* s) {
   for (void* p : s->buffers) cudaFree(p);
   s->buffers.clear();
@@ -630,40 +668,8 @@ extern "C" int mx_create(const mx_network* n, double drift, int device, mx_solve
     delete s;
     return MX_ERR_NETWORK;
   }
-  // shared-memory layout of one cell (doubles): A [ns][ld], kf kr, v (or G/RT), n, N Y F U K1-K4 dinv, red, ints
-  net.ld = ns | 1;  // odd: a column of A is read without bank conflicts
-  int off = 0;
-  auto take = [&](int doubles) {
-    const int o = off;
-    off += (doubles + 1) & ~1;
-    return o;
-  };
-  net.oA = take(ns * net.ld);
-  net.a_doubles = ns * net.ld;
-  net.oK = take(2 * nr + 2);
-  net.oV = take(std::max(nr + 1, ns + 1));
-  net.on = take(ns + 1);
-  net.oN = take(ns);
-  net.oY = take(ns);
-  net.oF = take(ns);
-  net.oU = take(ns);
-  net.oK1 = take(ns);
-  net.oK2 = take(ns);
-  net.oK3 = take(ns);
-  net.oK4 = take(ns);
-  net.oD = take(ns);
-  net.oRed = take(8);
-  net.oInts = take((ns + 8) / 2 + 1);
-  net.oPart = take(n->n_pieces);
-  {  // the guard's scratch: in the matrix's space past the staged atoms and input row when it fits there
-    const int staged = (ns * n->nel + ns + 1) & ~1;
-    if (staged + guard_scratch(ns) <= ns * net.ld)
-      net.oG = net.oA + staged;
-    else
-      net.oG = take(guard_scratch(ns));
-  }
-  net.doubles = off;
-  s->smem = (size_t)off * sizeof(double);
+  cell_layout(n, net);
+  s->smem = (size_t)net.doubles * sizeof(double);
 
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -1060,5 +1066,18 @@ extern "C" int mx_call_static(mx_solver* s, const double* x, const double* T, co
 extern "C" const char* mx_version(void) { return "maxichem_b200 0.1 sm_100a"; }
 
 extern "C" int mx_warps_per_cell(void) { return WARPS; }
+
+extern "C" int mx_cells_per_sm(const mx_network* n, int32_t device) {
+  if (!n || n->ns < 1 || n->ns > MX_MAX_SPECIES || n->nr < 0 || n->nr >= 2048 || n->nel < 1 ||
+      n->nel > MX_MAX_ELEMENTS)
+    return -MX_ERR_NETWORK;
+  Net net{};
+  cell_layout(n, net);
+  int per_sm = 0, reserved = 0;
+  if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) != cudaSuccess)
+    return -MX_ERR_CUDA;
+  return (int)((size_t)per_sm / ((size_t)net.doubles * sizeof(double) + (size_t)reserved));
+}
 
 extern "C" int mx_warps_supported(int32_t warps) { return warps == 2 || warps == 4 ? 1 : 0; }

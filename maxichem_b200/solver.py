@@ -30,6 +30,10 @@ INFO_FIELDS = ("warps", "rows_per_lane", "smem", "call_ctas_per_sm", "recover_ct
 PRECISIONS = {"fp64": 0, "mixed": 1}
 MIXED_TOL = 1.0  # MX_MIXED_TOL of include/maxichem_b200.h
 MAX_SWEEPS = 4  # MX_MIXED_MAX_SWEEPS
+# The default warps per cell is 2 when at least this many cells of the network fit one SM's shared memory: half again
+# the 4-warp kernels' 4 cells per SM (41 species: 2 warps measured 11-19 % faster; 69 species, 4 cells a SM either
+# way: 4 warps 16 % faster)
+TWO_WARP_CELLS = 6
 
 
 class CallResult(NamedTuple):
@@ -128,8 +132,10 @@ class CudaSolver:
     row-scaled FP32, every stage solve refined ``sweeps`` times against an FP64 residual; a try whose last correction
     exceeds ``tol`` times the error-control scale has its cell redone in FP64 in the same call, counted in
     ``escalated``). Results, counts, flags and refusals have the same meaning in both. ``warps``: warps per cell of
-    the call (4 by default, or 2: more cells per SM for small networks; the same results bit for bit; the
-    derivatives need 4).
+    the call, 2 or 4, the same results bit for bit; by default 2 for a network of which at least TWO_WARP_CELLS cells
+    fit one SM's shared memory (the 2-warp kernels then hold 6-8 cells per SM, registers allowing 8, against the
+    4-warp kernels' 4), else 4, as the reference chooses its warps per cell by the network's size
+    (maxichem/_constants.py:67-72) by its own rule. The derivatives need 4.
     """
 
     def __init__(self, net: VulcanNetwork, device: torch.device | str, *, drift: float | None = None,
@@ -154,10 +160,14 @@ class CudaSolver:
         self.net = net
         self.dev = _device_of(device)
         self._lib = abi.library()
-        self.warps = int(self._lib.mx_warps_per_cell()) if warps is None else int(warps)
+        tab = None
+        if warps is None:
+            self.warps, tab = self._default_warps(net, photo)
+        else:
+            self.warps = int(warps)
         if not self._lib.mx_warps_supported(self.warps):
             raise ValueError(f"warps: 2 or 4 warps per cell expected, got {warps}")
-        self.tab = tables.build(net, photo, warps=self.warps)
+        self.tab = tab if tab is not None else tables.build(net, photo, warps=self.warps)
         self.ns, self.nr, self.nj = self.tab.ns, self.tab.nr, self.tab.nj
         self.count = torch.zeros(abi.COUNT_SLOTS, dtype=torch.int32, device=self.dev)
         self.total = torch.zeros(abi.COUNT_SLOTS, dtype=torch.int64, device=self.dev)
@@ -176,6 +186,16 @@ class CudaSolver:
         self._lib.mx_set_escalation_counter(self._handle, self.escalated.data_ptr())
         self.info: dict[str, Any] = self.layout()
         self.info.update(ns=self.ns, nr=self.nr, nj=self.nj, drift=self.drift, flops=dict(self.tab.flops))
+
+    def _default_warps(self, net: VulcanNetwork, photo: bool) -> tuple[int, tables.Tables | None]:
+        """2 when at least TWO_WARP_CELLS cells of the network fit one SM's shared memory, else the library's default
+        (4); the tables already built for the choice, or None."""
+        four = int(self._lib.mx_warps_per_cell())
+        tab = tables.build(net, photo, warps=four)
+        cells = int(self._lib.mx_cells_per_sm(abi.NetworkStruct(tab).ref(), self.dev.index))
+        if cells >= TWO_WARP_CELLS and self._lib.mx_warps_supported(2):
+            return 2, None
+        return four, tab
 
     # lifetime (_solver.py:142-167)
     def close(self) -> None:

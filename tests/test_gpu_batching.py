@@ -144,3 +144,21 @@ def test_the_derivatives_refuse_two_warps(gpu, networks):
         assert len(args) == n
         assert lib.mx_jvp(*args) == 3  # MX_ERR_NETWORK
     assert b"4 warps per cell" in err.value
+
+
+def test_the_default_mapping_follows_the_network_size(gpu, networks):
+    # 41 species: a cell's shared memory lets at least 6 cells share an SM, so 2 warps by default; 69 and 91 species
+    # fit 4 or fewer, so 4 warps; the derivative solver takes 4 whatever the size
+    from maxichem_b200 import abi, tables
+    from maxichem_b200.ad import ADSolver
+    from maxichem_b200.solver import TWO_WARP_CELLS
+
+    lib = abi.library()
+    for name, want in (("cho41", 2), ("chno69", 4), ("sncho91", 4)):
+        net = networks(name)
+        with CudaSolver(net, gpu, photo=True) as s:
+            assert s.info["warps"] == want, name
+        cells = lib.mx_cells_per_sm(abi.NetworkStruct(tables.build(net, True, warps=4)).ref(), gpu.index or 0)
+        assert (cells >= TWO_WARP_CELLS) == (want == 2), (name, cells)
+    with ADSolver(networks("cho41"), gpu, photo=True) as ad:
+        assert ad.info["warps"] == 4
