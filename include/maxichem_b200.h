@@ -392,6 +392,15 @@ int mx_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int64_t
                  int32_t mode, const float* bias, float* z, int32_t ldz, void* out, int32_t ldo, int32_t* err_flag,
                  void* stream);
 
+/* The weight gradients' product alone (exported for tests): out[M][N] FP32 (pitch ldo) = A B^T as mx_gemm_bf16's
+ * mode 0, with K (the batch) split across the SMs when the output has fewer 128 x 64..256 tiles than the device has
+ * SMs: each split's partial product goes to workspace (mx_gemm_split_workspace(M, N, K) floats; NULL when that is 0)
+ * and a second kernel adds them in split order, so the result is the same bits run to run (not those of the unsplit
+ * product: the partial sums group the terms differently). */
+int mx_gemm_bf16_split(const void* A, int32_t lda, const void* B, int32_t ldb, int64_t M, int32_t N, int32_t K,
+                       float* workspace, float* out, int32_t ldo, int32_t* err_flag, void* stream);
+int64_t mx_gemm_split_workspace(int64_t M, int32_t N, int32_t K);
+
 /* Release the solver's device memory. Safe on NULL. */
 int mx_destroy(mx_solver* s);
 

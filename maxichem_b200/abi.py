@@ -172,6 +172,12 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
         [_P, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
          _P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, _P],
     ),  # fmt: skip
+    "mx_gemm_bf16_split": (
+        ctypes.c_int,
+        [_P, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P, _P,
+         ctypes.c_int32, _P, _P],
+    ),  # fmt: skip
+    "mx_gemm_split_workspace": (ctypes.c_int64, [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32]),
     "mx_set_escalation_counter": (ctypes.c_int, [_P, _P]),
     "mx_debug_try_mixed": (
         ctypes.c_int,

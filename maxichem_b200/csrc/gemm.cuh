@@ -43,7 +43,26 @@ struct Epi {
   void* out;          // [M][ldo]: FP32 (STORE, BIAS) or BF16 (BIAS_SILU, DSILU)
   int ldo;
   int tma;            // 1: out (and z) through the output tensor maps; 0: plain stores (unaligned out or z)
+  int splits;         // K split into this many consecutive ranges of 64-blocks (1: no split), each non-empty
+  int split_rows;     // rows of out between two splits' partial products (splits > 1: out is [splits][split_rows][ldo])
 };
+
+// Output tile t of a launch: rows m0.., columns n0.., K blocks kb0 .. kb1 - 1, output rows offset by orow. With
+// splits > 1 the tiles run split by split (consecutive CTAs share a split's K range of A and B in L2).
+struct Tile {
+  int m0, n0, kb0, kb1, orow;
+};
+template <int BN>
+__device__ __forceinline__ Tile tile_at(int t, int tiles_mn, int tiles_n, int nks, int nk, const Epi& ep) {
+  const int split = t / tiles_mn, tmn = t - split * tiles_mn;
+  Tile r;
+  r.m0 = (tmn / tiles_n) * BM;
+  r.n0 = (tmn % tiles_n) * BN;
+  r.kb0 = split * nks;
+  r.kb1 = min(nk, r.kb0 + nks);
+  r.orow = split * ep.split_rows;
+  return r;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -270,7 +289,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint64_t* bars = (uint64_t*)(stg + EPI_WARPS * STAGING);  // full[S], empty[S], acc_full[2], acc_empty[2], z[8]
   uint32_t* tslot = (uint32_t*)(bars + 2 * STAGES + 4 + EPI_WARPS);
   const int tid = (int)threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nk = K / BK, tiles_n = N / BN, tiles = ((M + BM - 1) / BM) * tiles_n;
+  const int nk = K / BK, tiles_n = N / BN, tiles_mn = ((M + BM - 1) / BM) * tiles_n;
+  const int nks = (nk + ep.splits - 1) / ep.splits, tiles = tiles_mn * ep.splits;
   const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES);
   const uint32_t accf0 = smem_u32(bars + 2 * STAGES), acce0 = smem_u32(bars + 2 * STAGES + 2);
   const uint32_t zbar0 = smem_u32(bars + 2 * STAGES + 4);
@@ -303,8 +323,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     long long kc = 0;
     bool ok = true;
     for (int t = (int)blockIdx.x; t < tiles && ok; t += (int)gridDim.x) {
-      const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
-      for (int kb = 0; kb < nk; kb++, kc++) {
+      const Tile tl = tile_at<BN>(t, tiles_mn, tiles_n, nks, nk, ep);
+      const int m0 = tl.m0, n0 = tl.n0;
+      for (int kb = tl.kb0; kb < tl.kb1; kb++, kc++) {
         const int s = (int)(kc % STAGES), r = (int)(kc / STAGES);
         if (r > 0 && !mbar_wait(empty0 + 8 * s, (uint32_t)((r - 1) & 1), err)) {
           ok = false;
@@ -328,7 +349,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (use > 0 && !mbar_wait(acce0 + 8 * acc, (uint32_t)((use - 1) & 1), err)) break;
       tmem_fence_after();
       const uint32_t d = tmem + (uint32_t)(acc * BN);
-      for (int kb = 0; kb < nk; kb++, kc++) {
+      const Tile tl = tile_at<BN>(t, tiles_mn, tiles_n, nks, nk, ep);
+      for (int kb = tl.kb0; kb < tl.kb1; kb++, kc++) {
         const int s = (int)(kc % STAGES), r = (int)(kc / STAGES);
         if (!mbar_wait(full0 + 8 * s, (uint32_t)(r & 1), err)) {
           ok = false;
@@ -339,7 +361,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const uint64_t db = sw128_desc(smem_u32(sb + s * BN * BK * 2));
 #pragma unroll
         for (int k = 0; k < BK / 16; k++)  // +32 bytes along K within the swizzled 128-byte rows: +2 in 16-byte units
-          umma_bf16(d, da + 2 * k, db + 2 * k, idesc, (kb > 0 || k > 0) ? 1u : 0u);
+          umma_bf16(d, da + 2 * k, db + 2 * k, idesc, (kb > tl.kb0 || k > 0) ? 1u : 0u);
         umma_commit(empty0 + 8 * s);
       }
       umma_commit(accf0 + 8 * acc);  // fires when this tile's MMAs (and every earlier one) have completed
@@ -358,7 +380,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     int i = 0;
     for (int t = (int)blockIdx.x; t < tiles && ok; t += (int)gridDim.x, i++) {
       const int acc = i & 1, use = i >> 1;
-      const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+      const Tile tl = tile_at<BN>(t, tiles_mn, tiles_n, nks, nk, ep);
+      const int m0 = tl.m0, n0 = tl.n0, orow = tl.orow;  // orow: the split's rows in out (split-K partials)
       const int r0 = m0 + 32 * quarter, row = r0 + lane;
       if (zin && tma) {  // this tile's first z piece, while the MMAs run
         if (lane == 0) {
@@ -434,13 +457,13 @@ __global__ void __launch_bounds__(THREADS, 1)
           fence_async_shared();
           __syncwarp();
           if (lane == 0 && r0 < M) {  // a piece wholly below the last row has nothing to store
-            tma_store_2d(&to, so_a, n0 + c, r0);
+            tma_store_2d(&to, so_a, n0 + c, r0 + orow);
             if (zout) tma_store_2d(&tz, sz_a, n0 + c, r0);
             bulk_commit();
           }
         } else if (row < M) {
           if (f32_out) {
-            float4* o = (float4*)((float*)ep.out + (size_t)row * ep.ldo + n0 + c);
+            float4* o = (float4*)((float*)ep.out + (size_t)(row + orow) * ep.ldo + n0 + c);
 #pragma unroll
             for (int q = 0; q < EPI_COLS / 4; q++)
               o[q] = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);

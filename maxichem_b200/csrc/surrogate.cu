@@ -89,7 +89,7 @@ cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, const CUte
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
   }
-  const long long tiles = ((M + BM - 1) / BM) * (long long)(N / BN);
+  const long long tiles = ((M + BM - 1) / BM) * (long long)(N / BN) * ep.splits;
   const int grid = (int)std::min<long long>(tiles, std::max(g_sms, 1));  // persistent: one CTA per SM
   gemm_kernel<BN, STAGES, EPI><<<grid, THREADS, smem, st>>>(ta, tb, to, tz, (int)M, N, K, ep, err);
   return cudaGetLastError();
@@ -112,7 +112,8 @@ cudaError_t launch_epi(int epi, const CUtensorMap& ta, const CUtensorMap& tb, co
 
 // C[M, N] = A[M, K] B[N, K]^T with the epilogue ep (gemm.cuh). Returns MX_ERR_ARGUMENT for shapes the kernel does not
 // take: K a multiple of 64, N of 64, 16-byte aligned pointers (A, B, out, bias, z) and row pitches (lda, ldb, ldo,
-// ldz in bytes).
+// ldz in bytes). ep.splits > 1 (STORE only): K in that many consecutive non-empty ranges, split s's partial product
+// in out's rows s * ep.split_rows .. (split_rows at least M rounded up to 128).
 int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, int N, int K, const Epi& ep, int* err,
                    cudaStream_t st) {
   const bool f32_out = ep.mode == STORE || ep.mode == BIAS;
@@ -123,6 +124,9 @@ int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, in
       ep.ldo % (f32_out ? 4 : 8) || (has_bias && (!ep.bias || ((uintptr_t)ep.bias & 15))) ||
       (uses_z && (!ep.z || ((uintptr_t)ep.z & 15) || ep.ldz < N || ep.ldz % 4)))
     return MX_ERR_ARGUMENT;
+  const int splits = std::max(ep.splits, 1), nk = K / BK, nks = (nk + splits - 1) / splits;
+  if (splits > 1 && (ep.mode != STORE || (splits - 1) * nks >= nk || ep.split_rows < (M + BM - 1) / BM * BM))
+    return MX_ERR_ARGUMENT;
   if (encoder() != cudaSuccess) return MX_ERR_CUDA;
   const int bn = N % 256 == 0 ? 256 : (N % 128 == 0 ? 128 : 64);  // the widest column tile that divides N
   CUtensorMap ta, tb, to, tz;
@@ -131,9 +135,12 @@ int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, in
     return MX_ERR_ARGUMENT;
   // the epilogue's outputs go through TMA stores when their maps can be made, else through plain stores
   Epi e2 = ep;
+  e2.splits = splits;
+  e2.split_rows = splits > 1 ? ep.split_rows : 0;
   memset(&to, 0, sizeof(to));
   memset(&tz, 0, sizeof(tz));
-  e2.tma = piece_map(&to, ep.out, (uint64_t)M, (uint64_t)N, (uint64_t)ep.ldo, f32_out) &&
+  const uint64_t out_rows = splits > 1 ? (uint64_t)splits * (uint64_t)ep.split_rows : (uint64_t)M;
+  e2.tma = piece_map(&to, ep.out, out_rows, (uint64_t)N, (uint64_t)ep.ldo, f32_out) &&
            (!uses_z || piece_map(&tz, ep.z, (uint64_t)M, (uint64_t)N, (uint64_t)ep.ldz, true));
   const int epi = variant_of(ep.mode, ep.mode == BIAS_SILU && ep.z != nullptr);
   const cudaError_t e = bn == 256   ? launch_epi<256, 3>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
@@ -142,11 +149,79 @@ int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, in
   return e == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
+namespace {
+
+// out[m][n] (pitch ldo) = the sum over s = 0 .. splits - 1, in that order, of ws[s * split_rows + m][n] (pitch n)
+__global__ void split_sum_kernel(const float* __restrict__ ws, int splits, int split_rows, int M, int N, float* out,
+                                 int ldo) {
+  const long long total = (long long)M * N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(i / N), n = (int)(i % N);
+    float acc = 0.0f;
+    for (int q = 0; q < splits; q++) acc += ws[((size_t)q * split_rows + m) * N + n];
+    out[(size_t)m * ldo + n] = acc;
+  }
+}
+
+// K split so that the launch has about one output tile per SM: 1 when the output alone fills the SMs
+int splits_for(int64_t M, int N, int K) {
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const int bn = N % 256 == 0 ? 256 : (N % 128 == 0 ? 128 : 64), nk = K / BK;
+  const long long tiles = ((M + BM - 1) / BM) * (long long)(N / bn);
+  const long long want = std::max<long long>(1, std::max(g_sms, 1) / std::max<long long>(tiles, 1));
+  if (want < 2 || nk < 2) return 1;
+  const int nks = (int)((nk + want - 1) / want);
+  return (nk + nks - 1) / nks;  // every split non-empty
+}
+
+}  // namespace
+
+// Floats of workspace a split-K product of this shape uses (0: it is not split).
+size_t mx_split_workspace(int64_t M, int N, int K) {
+  const int splits = splits_for(M, N, K);
+  return splits > 1 ? (size_t)splits * (size_t)((M + BM - 1) / BM * BM) * (size_t)N : 0;
+}
+
+// out[M][N] (FP32, pitch ldo) = A B^T with K split across the SMs when the output has fewer tiles than SMs: the
+// partial products go to ws (mx_split_workspace floats) and are added in split order by a second kernel, so the
+// result is the same bits run to run. The weight gradients' products (M, N the layer's sizes, K the batch) are this
+// shape: a few tiles, a long K.
+int mx_gemm_store_split(const void* A, int lda, const void* B, int ldb, int64_t M, int N, int K, float* ws,
+                        float* out, int ldo, int* err, cudaStream_t st) {
+  const int splits = splits_for(M, N, K);
+  if (splits == 1) {
+    Epi ep{STORE, nullptr, nullptr, 0, out, ldo, 0, 1, 0};
+    return mx_gemm_launch(A, lda, B, ldb, M, N, K, ep, err, st);
+  }
+  if (!ws || !out || ldo < N || ldo % 4 || ((uintptr_t)out & 15)) return MX_ERR_ARGUMENT;
+  const int rows = (int)((M + BM - 1) / BM * BM);
+  Epi ep{STORE, nullptr, nullptr, 0, ws, N, 0, splits, rows};
+  const int rc = mx_gemm_launch(A, lda, B, ldb, M, N, K, ep, err, st);
+  if (rc) return rc;
+  const int grid = (int)std::min<long long>((M * (long long)N + 255) / 256, 148LL * 64);
+  split_sum_kernel<<<grid, 256, 0, st>>>(ws, splits, rows, (int)M, N, out, ldo);
+  return cudaGetLastError() == cudaSuccess ? MX_OK : MX_ERR_CUDA;
+}
+
+extern "C" int mx_gemm_bf16_split(const void* A, int32_t lda, const void* B, int32_t ldb, int64_t M, int32_t N,
+                                  int32_t K, float* workspace, float* out, int32_t ldo, int32_t* err_flag,
+                                  void* stream) {
+  return mx_gemm_store_split(A, lda, B, ldb, M, N, K, workspace, out, ldo, err_flag, (cudaStream_t)stream);
+}
+
+extern "C" int64_t mx_gemm_split_workspace(int64_t M, int32_t N, int32_t K) {
+  return (int64_t)mx_split_workspace(M, N, K);
+}
+
 extern "C" int mx_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int64_t M, int32_t N, int32_t K,
                             int32_t mode, const float* bias, float* z, int32_t ldz, void* out, int32_t ldo,
                             int32_t* err_flag, void* stream) {
   if (mode < STORE || mode > DSILU) return MX_ERR_ARGUMENT;
-  Epi ep{mode, bias, z, ldz, out, ldo, 0};
+  Epi ep{mode, bias, z, ldz, out, ldo, 0, 1, 0};
   return mx_gemm_launch(A, lda, B, ldb, M, N, K, ep, err_flag, (cudaStream_t)stream);
 }
 
@@ -583,6 +658,7 @@ struct mx_surrogate {
   float* pred = nullptr;
   __nv_bfloat16 *dz = nullptr, *dz2 = nullptr, *dzt = nullptr, *at = nullptr;
   float* colpart = nullptr;
+  float* ws = nullptr;  // split-K partial products of the weight gradients
   // the gated call's workspace for up to `call_rows` cells
   int64_t call_rows = 0;
   std::vector<void*> call_work;
@@ -643,6 +719,9 @@ cudaError_t grow_train(mx_surrogate* s, int64_t M) {
   if (e == cudaSuccess) e = alloc(s->work, &s->dzt, (size_t)M * wide);
   if (e == cudaSuccess) e = alloc(s->work, &s->at, (size_t)M * wide);
   if (e == cudaSuccess) e = alloc(s->work, &s->colpart, (size_t)64 * wide);
+  size_t ws = 0;
+  for (int l = 0; l <= s->layers; l++) ws = std::max(ws, mx_split_workspace(s->L.rows[l], s->L.cols[l], (int)M));
+  if (e == cudaSuccess && ws) e = alloc(s->work, &s->ws, ws);
   if (e == cudaSuccess) s->rows = M;
   return e;
 }
@@ -833,8 +912,8 @@ extern "C" int mx_sur_train_step(mx_surrogate* s, const void* feat, const float*
     const dim3 tb(32, 8);
     transpose_kernel<<<dim3((N + 31) / 32, (unsigned)((M + 31) / 32)), tb, 0, st>>>(dZ, (int)M, N, s->dzt);
     transpose_kernel<<<dim3((K + 31) / 32, (unsigned)((M + 31) / 32)), tb, 0, st>>>(a, (int)M, K, s->at);
-    Epi gw{STORE, nullptr, nullptr, 0, s->grad + s->L.w_off[l], K};
-    rc = mx_gemm_launch(s->dzt, (int)M, s->at, (int)M, N, K, (int)M, gw, s->err, st);
+    rc = mx_gemm_store_split(s->dzt, (int)M, s->at, (int)M, N, K, (int)M, s->ws, s->grad + s->L.w_off[l], K, s->err,
+                             st);
     if (rc) return rc;
     const int chunks = (int)std::min<int64_t>(64, (M + 127) / 128), per = (int)((M + chunks - 1) / chunks);
     colsum_part_kernel<<<dim3((N + 31) / 32, chunks), tb, 0, st>>>(dZ, (int)M, N, per, s->colpart);

@@ -91,3 +91,33 @@ def test_unaligned_outputs_bias_or_z_are_refused(gpu):
     assert p(DSILU, None, z.data_ptr() + 8, N, out.data_ptr(), N) == 1     # z 8 bytes off
     torch.cuda.synchronize(gpu)
     assert bool((out == 7.0).all()) and bool((z == 7.0).all())
+
+
+@pytest.mark.parametrize("M,N,K", [(512, 512, 16384), (320, 512, 8192), (512, 128, 4096), (128, 64, 128)])
+def test_the_split_k_product_matches_the_unsplit_one(gpu, M, N, K):
+    """The weight gradients' shape (a few output tiles, a long K): K split across the SMs, the partial products
+    added in split order by a second kernel; against the FP32 product, and the same bits twice."""
+    g = torch.Generator(device=gpu)
+    g.manual_seed(M + N + K + 1)
+    A = torch.randn(M, K, device=gpu, generator=g).to(torch.bfloat16)
+    B = (torch.randn(N, K, device=gpu, generator=g) / K**0.5).to(torch.bfloat16)
+    ref = A.float() @ B.float().T
+    lib = abi.library()
+    n_ws = lib.mx_gemm_split_workspace(M, N, K)
+    if (M, N, K) != (128, 64, 128):
+        assert n_ws > 0  # these shapes do split
+    ws = torch.full((max(n_ws, 1),), float("nan"), device=gpu)
+    flag = torch.zeros(1, dtype=torch.int32, device=gpu)
+    outs = []
+    for _ in range(2):
+        out = torch.full((M, N + 4), float("nan"), device=gpu)
+        rc = lib.mx_gemm_bf16_split(A.data_ptr(), K, B.data_ptr(), K, M, N, K, ws.data_ptr() if n_ws else None,
+                                    out.data_ptr(), N + 4, flag.data_ptr(), None)  # fmt: skip
+        assert rc == 0
+        torch.cuda.synchronize(gpu)
+        assert int(flag.item()) == 0
+        outs.append(out)
+    got = outs[0][:, :N]
+    assert float((got - ref).abs().max()) <= 2e-5 * float(ref.abs().max()) + 1e-6 * K**0.5
+    assert torch.equal(outs[0][:, :N], outs[1][:, :N])
+    assert bool(torch.isnan(outs[0][:, N:]).all())
