@@ -67,7 +67,9 @@ def parse() -> argparse.Namespace:
     p.add_argument("--arms", default="fp64,learned",
                    help="comma list of fp64, learned (the surrogate's gated call), mixed (FP32 factors)")
     p.add_argument("--train-cells", type=int, default=1 << 20, help="cells of the surrogate's training pairs")
-    p.add_argument("--train-calls", type=int, default=6, help="chained calls of the training pairs")
+    p.add_argument("--train-calls", type=int, default=10,
+                   help="chained calls of the training pairs (10 x 1,048,576 cells: the 10 M pairs of the surrogate's "
+                        "configuration)")
     p.add_argument("--epochs", type=int, default=20, help="training epochs of the surrogate")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")

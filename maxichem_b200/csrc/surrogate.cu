@@ -309,18 +309,25 @@ __global__ void loss_grad_kernel(const float* pred, int ldp, const float* tgt, c
   if (threadIdx.x == 0 && loss) atomicAdd(loss, part[0] * scale);
 }
 
-// out [C][R] = in [R][C] (BF16), 32 x 32 tiles through shared memory.
+// out [C][R] = in [R][C] (BF16; R and C even, rows 4-byte aligned), 64 x 64 tiles through shared memory: each warp
+// reads and writes 128 contiguous bytes of a row as 32 pairs; the tile's odd row stride (65 elements) keeps the
+// column reads free of bank conflicts.
 __global__ void transpose_kernel(const __nv_bfloat16* in, int R, int C, __nv_bfloat16* out) {
-  __shared__ __nv_bfloat16 tile[32][34];
-  const int c0 = (int)blockIdx.x * 32, r0 = (int)blockIdx.y * 32, tx = (int)threadIdx.x, ty = (int)threadIdx.y;
-  for (int k = ty; k < 32; k += 8) {
-    const int r = r0 + k, c = c0 + tx;
-    tile[k][tx] = (r < R && c < C) ? in[(size_t)r * C + c] : __float2bfloat16_rn(0.0f);
+  __shared__ __nv_bfloat16 tile[64][65];
+  const int c0 = (int)blockIdx.x * 64, r0 = (int)blockIdx.y * 64, tx = (int)threadIdx.x, ty = (int)threadIdx.y;
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+  for (int k = ty; k < 64; k += 8) {
+    const int r = r0 + k, c = c0 + 2 * tx;
+    __nv_bfloat162 v = __halves2bfloat162(zero, zero);
+    if (r < R && c < C) v = *reinterpret_cast<const __nv_bfloat162*>(in + (size_t)r * C + c);  // c + 1 < C: C even
+    tile[k][2 * tx] = v.x;
+    tile[k][2 * tx + 1] = v.y;
   }
   __syncthreads();
-  for (int k = ty; k < 32; k += 8) {
-    const int c = c0 + k, r = r0 + tx;
-    if (c < C && r < R) out[(size_t)c * R + r] = tile[tx][k];
+  for (int k = ty; k < 64; k += 8) {
+    const int c = c0 + k, r = r0 + 2 * tx;
+    if (c < C && r < R)  // r + 1 < R: R even
+      *reinterpret_cast<__nv_bfloat162*>(out + (size_t)c * R + r) = __halves2bfloat162(tile[2 * tx][k], tile[2 * tx + 1][k]);
   }
 }
 
@@ -910,8 +917,8 @@ extern "C" int mx_sur_train_step(mx_surrogate* s, const void* feat, const float*
     const __nv_bfloat16* a = l == 0 ? f : s->act[l];
     const int K = s->L.cols[l];
     const dim3 tb(32, 8);
-    transpose_kernel<<<dim3((N + 31) / 32, (unsigned)((M + 31) / 32)), tb, 0, st>>>(dZ, (int)M, N, s->dzt);
-    transpose_kernel<<<dim3((K + 31) / 32, (unsigned)((M + 31) / 32)), tb, 0, st>>>(a, (int)M, K, s->at);
+    transpose_kernel<<<dim3((N + 63) / 64, (unsigned)((M + 63) / 64)), tb, 0, st>>>(dZ, (int)M, N, s->dzt);
+    transpose_kernel<<<dim3((K + 63) / 64, (unsigned)((M + 63) / 64)), tb, 0, st>>>(a, (int)M, K, s->at);
     rc = mx_gemm_store_split(s->dzt, (int)M, s->at, (int)M, N, K, (int)M, s->ws, s->grad + s->L.w_off[l], K, s->err,
                              st);
     if (rc) return rc;
