@@ -432,7 +432,7 @@ def mlp_roofline(sur, x, T, P, dt, h, J, stream) -> dict:
 
     feat, _ = sur.features(x, T, P, dt, h, J)
     ms, _ = timed_steps(lambda: sur.forward(feat), 5, 2, stream)
-    flop = 2.0 * feat.shape[0] * sum(r * c for r, c in sur.shapes)
+    flop = 2.0 * feat.shape[0] * useful_macs(sur)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak, sustained = peaks.get("bf16_tflops", 1590.0), peaks.get("bf16_tflops_sustained", 1400.0)
     torch.cuda.synchronize()
@@ -440,6 +440,15 @@ def mlp_roofline(sur, x, T, P, dt, h, J, stream) -> dict:
             "peak": peak, "unit": "TFLOP/s", "frac": flop / ms / 1e9 / peak, "frac_of_sustained": flop / ms / 1e9 /
             sustained, "ms_per_forward": ms, "flops_per_forward": flop,
             "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst: the forward's launches timed alone)"}  # fmt: skip
+
+
+def useful_macs(sur) -> int:
+    """Multiply-adds per row of the network's forward pass on its real sizes: the features (not their padding to a
+    multiple of 64) into the first layer, the heads' real outputs (not their padding to a 128- or 192-wide tile)."""
+    sizes = [(r, c) for r, c in sur.shapes]
+    sizes[0] = (sizes[0][0], sur.nf)
+    sizes[-1] = (sur.heads * sur.nt, sizes[-1][1])
+    return sum(r * c for r, c in sizes)
 
 
 def run_mlp(args) -> None:
@@ -474,7 +483,7 @@ def run_mlp(args) -> None:
         ms_train, _ = timed_steps(lambda: sur.train_step(feat, tgt, wts, 1e-4, delta=1.0), args.steps, args.warmup,
                                   stream)  # fmt: skip
     sur.check()
-    flop = 2.0 * rows * sum(r * c for r, c in sur.shapes)
+    flop = 2.0 * rows * useful_macs(sur)  # the padding's multiply-adds are done but not counted
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("bf16_tflops", 1590.0)
     achieved = flop / ms_fwd / 1e9

@@ -216,6 +216,13 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// TMEM columns of the two accumulators: 2 BN rounded up to a power of two (an allocation's size), at most 512.
+__host__ __device__ constexpr uint32_t tmem_columns(int bn) {
+  uint32_t c = 32;
+  while (c < 2u * (uint32_t)bn) c <<= 1;
+  return c;
+}
+
 // Shared-memory bytes of one CTA: the stages (1024-aligned), the epilogue warps' staging, the barriers and the TMEM
 // address slot, plus the slack that aligns the dynamic base to 1024 bytes.
 template <int BN, int STAGES>
@@ -307,9 +314,10 @@ __global__ void __launch_bounds__(THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  if (warp == 1) {  // two accumulators of BN columns (2 BN a power of two >= 32, at most 512)
+  constexpr uint32_t TMEM_COLS = tmem_columns(BN);
+  if (warp == 1) {  // two accumulators of BN columns, in the power of two of columns at or above 2 BN
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                 "r"(2 * BN)
+                 "r"(TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -522,7 +530,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   __syncthreads();
   if (warp == 1) {
     tmem_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
   }
 }
 

@@ -13,6 +13,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -72,17 +73,24 @@ bool piece_map(CUtensorMap* m, const void* p, uint64_t rows, uint64_t cols, uint
 
 int g_sms = 0;
 
+// the column tile of a product with N columns: the widest of 256, 192, 128, 64 that divides N
+int tile_width(int N) { return N % 256 == 0 ? 256 : N % 192 == 0 ? 192 : N % 128 == 0 ? 128 : 64; }
+
 template <int BN, int STAGES, int EPI>
 cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& to, const CUtensorMap& tz,
                         int64_t M, int N, int K, const Epi& ep, int* err, cudaStream_t st) {
-  static bool configured = false;  // per instance: the opt-in shared memory
+  // the opt-in shared memory, set once per instance and device (a bit per device; devices past 63 set it every time)
+  static std::atomic<unsigned long long> configured{0};
   constexpr int smem = gemm_smem_bytes<BN, STAGES>();
   static_assert(smem <= 232448, "more shared memory than a CTA of sm_100a may opt into");
-  if (!configured) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return cudaErrorInvalidDevice;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (!bit || !(configured.load() & bit)) {
     const cudaError_t e = cudaFuncSetAttribute((const void*)gemm_kernel<BN, STAGES, EPI>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    configured = true;
+    configured.fetch_or(bit);
   }
   if (!g_sms) {
     int dev = 0;
@@ -128,7 +136,7 @@ int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, in
   if (splits > 1 && (ep.mode != STORE || (splits - 1) * nks >= nk || ep.split_rows < (M + BM - 1) / BM * BM))
     return MX_ERR_ARGUMENT;
   if (encoder() != cudaSuccess) return MX_ERR_CUDA;
-  const int bn = N % 256 == 0 ? 256 : (N % 128 == 0 ? 128 : 64);  // the widest column tile that divides N
+  const int bn = tile_width(N);
   CUtensorMap ta, tb, to, tz;
   if (!tensor_map(&ta, A, (uint64_t)M, (uint64_t)K, (uint64_t)lda, BM) ||
       !tensor_map(&tb, B, (uint64_t)N, (uint64_t)K, (uint64_t)ldb, (uint32_t)bn))
@@ -144,6 +152,7 @@ int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, in
            (!uses_z || piece_map(&tz, ep.z, (uint64_t)M, (uint64_t)N, (uint64_t)ep.ldz, true));
   const int epi = variant_of(ep.mode, ep.mode == BIAS_SILU && ep.z != nullptr);
   const cudaError_t e = bn == 256   ? launch_epi<256, 3>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
+                        : bn == 192 ? launch_epi<192, 4>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
                         : bn == 128 ? launch_epi<128, 5>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
                                     : launch_epi<64, 7>(epi, ta, tb, to, tz, M, N, K, e2, err, st);
   return e == cudaSuccess ? MX_OK : MX_ERR_CUDA;
@@ -170,7 +179,7 @@ int splits_for(int64_t M, int N, int K) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
   }
-  const int bn = N % 256 == 0 ? 256 : (N % 128 == 0 ? 128 : 64), nk = K / BK;
+  const int bn = tile_width(N), nk = K / BK;
   const long long tiles = ((M + BM - 1) / BM) * (long long)(N / bn);
   const long long want = std::max<long long>(1, std::max(g_sms, 1) / std::max<long long>(tiles, 1));
   if (want < 2 || nk < 2) return 1;
@@ -642,6 +651,13 @@ __global__ void audit_kernel(const int* cells, const int* count, int cap, const 
 
 int round64(int v) { return (v + 63) / 64 * 64; }
 
+// The heads' padded width: the first multiple of 64 at or above v that a 128-, 192- or 256-column tile divides, so
+// that their GEMM runs in wide tiles (A, the 65,536-row activations, is read once per column tile).
+int heads_width(int v) {
+  for (int w = round64(v);; w += 64)
+    if (w % 128 == 0 || w % 192 == 0) return w;
+}
+
 }  // namespace
 
 struct mx_surrogate {
@@ -779,7 +795,7 @@ extern "C" int mx_sur_create(int32_t ns, int32_t nj, int32_t nel, const double* 
   s->nf = ns + 4 + nj;
   s->kin = round64(s->nf);
   s->nt = ns + 1;
-  s->kout = round64(heads * s->nt);
+  s->kout = heads_width(heads * s->nt);
   Layers& L = s->L;
   L.n = layers + 1;
   long long off = 0, woff = 0;

@@ -1,6 +1,6 @@
 """The surrogate's tcgen05 BF16 GEMM (mx_gemm_bf16) against a plain PyTorch FP32 computation on the same BF16
-operands: every epilogue, full and partial row tiles, the three column tile widths (64, 128, 256), several K, and a
-shape with many tiles per persistent CTA."""
+operands: every epilogue, full and partial row tiles, the four column tile widths (64, 128, 192, 256), several K,
+and a shape with many tiles per persistent CTA."""
 
 import numpy as np
 import pytest
@@ -33,8 +33,9 @@ def run(mode, A, B, bias=None, z=None):
 
 
 # (65536, 512, 512): 1,024 tiles over the persistent CTAs (one per SM), so each CTA reuses both accumulators many times
+# (20000, 192, 256), (300, 384, 128): 192-column tiles (TMEM accumulators rounded up to 512 columns)
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 128, 512), (1000, 320, 512), (4096, 512, 128), (77, 64, 192),
-                                   (65536, 512, 512), (20000, 192, 256)])
+                                   (65536, 512, 512), (20000, 192, 256), (300, 384, 128), (65536, 384, 512)])
 def test_every_epilogue_matches_an_fp32_product(gpu, M, N, K):
     g = torch.Generator(device=gpu)
     g.manual_seed(M + N + K)
