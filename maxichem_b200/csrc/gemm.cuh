@@ -3,9 +3,9 @@
 // C[M, N] = A[M, K] B[N, K]^T, A and B row-major BF16 (both K-major), FP32 accumulation in tensor memory, in tiles of
 // 128 x BN: TMA streams the K blocks of A and B into shared-memory stages (128-byte swizzle, tensor maps over this
 // GPU's memory only), one thread issues the tcgen05.mma's (M 128, N BN, K 16 each, four per 64-wide K block) into a
-// TMEM accumulator and hands each stage back with tcgen05.commit, and eight warps read the accumulator (tcgen05.ld
-// 32x32b) through the epilogue, which stages each 32-row x 32-column piece of its outputs in shared memory (64- or
-// 128-byte swizzle, conflict-free for the row-per-lane writes) and writes it with a TMA store. Every wait on an mbarrier
+// TMEM accumulator and hands each stage back with tcgen05.commit, and 8 or 16 warps read the accumulator (tcgen05.ld
+// 32x32b) through the epilogue, which stages each 32-row piece of its outputs in shared memory (32-, 64- or 128-byte
+// swizzle, conflict-free for the row-per-lane writes) and writes it with a TMA store. Every wait on an mbarrier
 // gives up after about a second of clock ticks: the CTA then sets *err, lets its issued copies finish (bounded waits),
 // frees its tensor memory and returns.
 //
@@ -21,12 +21,17 @@
 namespace mxg {
 
 constexpr int BM = 128, BK = 64;
-constexpr int EPI_WARPS = 8;                  // two per TMEM lane quarter, each over half the tile's columns
-constexpr int THREADS = 64 + 32 * EPI_WARPS;  // producer warp, MMA warp, epilogue warps
-constexpr int EPI_COLS = 32;                  // accumulator columns per epilogue step
-// per epilogue warp: the output piece at 0 (32 x 32 FP32, 4 KB, or BF16, 2 KB) and the z piece at 2 KB (FP32, 4 KB);
-// the FP32 outputs (STORE, BIAS) have no z, so the two never overlap in use
-constexpr int STAGING = 6144;
+// The epilogue's shape for EW epilogue warps: 8, two per TMEM lane quarter in 32-column steps, or 16, four per quarter
+// in 16-column steps (half the registers, so that four epilogue warps share each SM sub-partition). Per warp, the
+// staging holds the output piece at 0 (32 rows x COLS FP32, or BF16) and the z piece at 2 KB (FP32); the FP32 outputs
+// (STORE, BIAS) have no z, so the two never overlap in use.
+template <int EW>
+struct EpiShape {
+  static_assert(EW == 8 || EW == 16, "8 or 16 epilogue warps");
+  static constexpr int THREADS = 64 + 32 * EW;  // producer warp, MMA warp, epilogue warps
+  static constexpr int COLS = EW == 8 ? 32 : 16;
+  static constexpr int STAGING = EW == 8 ? 6144 : 4096;
+};
 enum Epilogue { STORE = 0, BIAS = 1, BIAS_SILU = 2, DSILU = 3 };
 // The kernel is compiled per epilogue (its registers then hold only what that epilogue needs): BIAS_SILU splits into
 // SILU (activation only, the inference pass) and SILU_Z (the pre-activation kept in FP32 too, the training pass).
@@ -155,9 +160,24 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 __device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
-// 32 consecutive accumulator columns of the warp's 32 TMEM lanes (one row per thread), issued; tmem_wait32 waits for
-// every load of the thread and ties v's registers to the wait, so that no use of them moves above it.
-__device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&v)[32]) {
+// 32 (or 16) consecutive accumulator columns of the warp's 32 TMEM lanes (one row per thread), issued; tmem_wait waits
+// for every load of the thread and ties v's registers to the wait, so that no use of them moves above it.
+__device__ __forceinline__ void tmem_load(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait(uint32_t (&v)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                 "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void tmem_load(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
       "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
@@ -167,7 +187,7 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&v)[32]) {
         "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
 }
-__device__ __forceinline__ void tmem_wait32(uint32_t (&v)[32]) {
+__device__ __forceinline__ void tmem_wait(uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;"
                : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
                  "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]),
@@ -225,20 +245,22 @@ __host__ __device__ constexpr uint32_t tmem_columns(int bn) {
 
 // Shared-memory bytes of one CTA: the stages (1024-aligned), the epilogue warps' staging, the barriers and the TMEM
 // address slot, plus the slack that aligns the dynamic base to 1024 bytes.
-template <int BN, int STAGES>
+template <int BN, int STAGES, int EW>
 __host__ __device__ constexpr int gemm_smem_bytes() {
-  return STAGES * (BM + BN) * BK * 2 + EPI_WARPS * STAGING + 8 * (2 * STAGES + 4 + EPI_WARPS) + 16 + 1024;
+  return STAGES * (BM + BN) * BK * 2 + EW * EpiShape<EW>::STAGING + 8 * (2 * STAGES + 4 + EW) + 16 + 1024;
 }
 
-// Byte offsets of 16-byte chunk c of row r in the staging pieces, as the TMA unit lays out a swizzled box: 64-byte rows
-// (32 BF16) with the 64-byte swizzle, 128-byte rows (32 FP32) with the 128-byte swizzle (chunk index XOR address bits
-// 7 and up). Eight consecutive lanes writing chunk c of their rows then hit eight different 16-byte bank groups.
-__device__ __forceinline__ uint32_t sw64_at(int r, int c) { return (uint32_t)(r * 64 + ((c ^ ((r >> 1) & 3)) << 4)); }
-__device__ __forceinline__ uint32_t sw128_at(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
+// Byte offset of 16-byte chunk c of row r in a staging piece of RB-byte rows (32, 64 or 128) as the TMA unit lays out
+// a box with the RB-byte swizzle: the chunk index XOR the address bits 7 and up. Eight consecutive lanes writing chunk
+// c of their rows then hit eight different 16-byte bank groups.
+template <int RB>
+__device__ __forceinline__ uint32_t swz(int r, int c) {
+  return (uint32_t)(r * RB + ((c ^ ((r * RB >> 7) & (RB / 16 - 1))) << 4));
+}
 
-// The epilogue's arithmetic on 32 accumulator columns (a[32], columns col .. col + 31) of one row; zz holds z for
-// DSILU. BIAS_SILU leaves z = C + bias in zz and the activation in a.
-template <int EPI, int SFU_EVERY>
+// The epilogue's arithmetic on COLS accumulator columns (a, columns col ..) of one row; zz holds z for DSILU.
+// BIAS_SILU leaves z = C + bias in zz and the activation in a.
+template <int EPI, int SFU_EVERY, int EPI_COLS>
 __device__ __forceinline__ void epilogue_math(const Epi& ep, float (&a)[EPI_COLS], float (&zz)[EPI_COLS], int col) {
   if constexpr (EPI == V_BIAS || EPI == V_SILU || EPI == V_SILU_Z) {
     const float4* b4 = reinterpret_cast<const float4*>(ep.bias + col);
@@ -266,6 +288,7 @@ __device__ __forceinline__ void epilogue_math(const Epi& ep, float (&a)[EPI_COLS
   }
 }
 
+template <int EPI_COLS>
 __device__ __forceinline__ void pack_bf16(const float (&a)[EPI_COLS], uint32_t (&p)[EPI_COLS / 2]) {
 #pragma unroll
   for (int j = 0; j < EPI_COLS / 2; j++) {
@@ -274,17 +297,18 @@ __device__ __forceinline__ void pack_bf16(const float (&a)[EPI_COLS], uint32_t (
   }
 }
 
-// Persistent and warp-specialised: one CTA of 10 warps per SM walks the output tiles (row tiles outer, column tiles
-// inner, so neighbouring tiles share A's rows in L2). Warp 0 (one thread) streams the K blocks of A and B into a ring
-// of STAGES shared-memory stages; warp 1 (one thread) issues the MMAs into one of two TMEM accumulators of BN columns
-// each and commits; warps 2-9 drain the other accumulator through the epilogue (warp w the TMEM lanes 32 (w % 4) ..
-// 32 (w % 4) + 31, warps 2-5 the left half of the columns and 6-9 the right half) and hand it back, so a tile's
-// epilogue overlaps the next tile's MMAs. With ep.tma, each epilogue warp stages its 32 x 32 output pieces in its own
-// 6 KB of shared memory and stores them with TMA (one bulk group per warp, waited for before the staging is rewritten);
-// DSILU's z pieces come in the same way by TMA loads, one ahead. EPI is the epilogue (Variant); SFU_EVERY sets the
-// sigmoid's split between the special-function unit and the FMA pipe.
-template <int BN, int STAGES, int EPI, int SFU_EVERY = 2>
-__global__ void __launch_bounds__(THREADS, 1)
+// Persistent and warp-specialised: one CTA of 2 + EW warps per SM walks the output tiles (row tiles outer, column
+// tiles inner, so neighbouring tiles share A's rows in L2). Warp 0 (one thread) streams the K blocks of A and B into a
+// ring of STAGES shared-memory stages; warp 1 (one thread) issues the MMAs into one of two TMEM accumulators of BN
+// columns each and commits; warps 2 .. EW + 1 drain the other accumulator through the epilogue (warp w the TMEM lanes
+// 32 (w % 4) .. 32 (w % 4) + 31; the EW / 4 warps of a lane quarter take consecutive slices of the columns) and hand
+// it back, so a tile's epilogue overlaps the next tile's MMAs. With ep.tma, each epilogue warp stages its 32-row
+// output pieces in its own shared memory and stores them with TMA (one bulk group per warp, waited for before the
+// staging is rewritten); DSILU's z pieces come in the same way by TMA loads, one ahead. EPI is the epilogue
+// (Variant); EW the epilogue warps (EpiShape); SFU_EVERY the sigmoid's split between the special-function unit and
+// the FMA pipe.
+template <int BN, int STAGES, int EPI, int EW, int SFU_EVERY = 2>
+__global__ void __launch_bounds__(EpiShape<EW>::THREADS, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
                 const __grid_constant__ CUtensorMap to, const __grid_constant__ CUtensorMap tz, int M, int N, int K,
                 Epi ep, int* err) {
@@ -292,9 +316,10 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint8_t* base = (uint8_t*)(((uintptr_t)gemm_smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* sa = base;                                       // STAGES x [128][64] BF16
   uint8_t* sb = base + STAGES * BM * BK * 2;                // STAGES x [BN][64] BF16
-  uint8_t* stg = sb + STAGES * BN * BK * 2;                 // EPI_WARPS x STAGING
-  uint64_t* bars = (uint64_t*)(stg + EPI_WARPS * STAGING);  // full[S], empty[S], acc_full[2], acc_empty[2], z[8]
-  uint32_t* tslot = (uint32_t*)(bars + 2 * STAGES + 4 + EPI_WARPS);
+  constexpr int EPI_COLS = EpiShape<EW>::COLS, STAGING = EpiShape<EW>::STAGING;
+  uint8_t* stg = sb + STAGES * BN * BK * 2;          // EW x STAGING
+  uint64_t* bars = (uint64_t*)(stg + EW * STAGING);  // full[S], empty[S], acc_full[2], acc_empty[2], z[EW]
+  uint32_t* tslot = (uint32_t*)(bars + 2 * STAGES + 4 + EW);
   const int tid = (int)threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nk = K / BK, tiles_n = N / BN, tiles_mn = ((M + BM - 1) / BM) * tiles_n;
   const int nks = (nk + ep.splits - 1) / ep.splits, tiles = tiles_mn * ep.splits;
@@ -308,9 +333,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(accf0 + 8 * b, 1);
-      mbar_init(acce0 + 8 * b, EPI_WARPS);  // one arrival per epilogue warp
+      mbar_init(acce0 + 8 * b, EW);  // one arrival per epilogue warp
     }
-    for (int w = 0; w < EPI_WARPS; w++) mbar_init(zbar0 + 8 * w, 1);
+    for (int w = 0; w < EW; w++) mbar_init(zbar0 + 8 * w, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -376,9 +401,12 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
   } else if (warp >= 2) {  // epilogue
     const int ew = warp - 2, quarter = warp & 3;
-    const int cbeg = (ew >> 2) * (BN / 2), cend = cbeg + BN / 2;
-    uint8_t* so = stg + ew * STAGING;  // output piece: 32 rows x 64 B (BF16) or 128 B (FP32)
-    uint8_t* sz = so + 2048;           // z piece: 32 rows x 128 B (FP32)
+    constexpr int WCOLS = BN * 4 / EW;  // columns of the warp's slice
+    static_assert(WCOLS % EPI_COLS == 0, "the slice is whole steps");
+    constexpr int RB16 = EPI_COLS * 2, RB32 = EPI_COLS * 4;  // staging row bytes: BF16 and FP32 pieces
+    const int cbeg = (ew >> 2) * WCOLS, cend = cbeg + WCOLS;
+    uint8_t* so = stg + ew * STAGING;  // output piece: 32 rows x RB16 (BF16) or RB32 (FP32)
+    uint8_t* sz = so + 2048;           // z piece: 32 rows x RB32 (FP32)
     const uint32_t so_a = smem_u32(so), sz_a = smem_u32(sz), zbar = zbar0 + 8 * ew;
     constexpr bool f32_out = EPI == V_STORE || EPI == V_BIAS, zout = EPI == V_SILU_Z, zin = EPI == V_DSILU;
     const bool tma = ep.tma != 0;
@@ -411,7 +439,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             z_done++;
 #pragma unroll
             for (int q = 0; q < EPI_COLS / 4; q++) {
-              const float4 z4 = *reinterpret_cast<const float4*>(sz + sw128_at(lane, q));
+              const float4 z4 = *reinterpret_cast<const float4*>(sz + swz<RB32>(lane, q));
               zz[4 * q] = z4.x;
               zz[4 * q + 1] = z4.y;
               zz[4 * q + 2] = z4.z;
@@ -429,7 +457,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
           }
         }
-        epilogue_math<EPI, SFU_EVERY>(ep, a, zz, n0 + c);
+        epilogue_math<EPI, SFU_EVERY, EPI_COLS>(ep, a, zz, n0 + c);
         if (zin && tma) {  // the z piece is consumed: fetch the next one into the same staging
           __syncwarp();
           if (c + EPI_COLS < cend) {
@@ -446,20 +474,20 @@ __global__ void __launch_bounds__(THREADS, 1)
           if (f32_out) {
 #pragma unroll
             for (int q = 0; q < EPI_COLS / 4; q++)
-              *reinterpret_cast<float4*>(so + sw128_at(lane, q)) =
+              *reinterpret_cast<float4*>(so + swz<RB32>(lane, q)) =
                   make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
           } else {
             uint32_t p[EPI_COLS / 2];
             pack_bf16(a, p);
 #pragma unroll
             for (int q = 0; q < EPI_COLS / 8; q++)
-              *reinterpret_cast<uint4*>(so + sw64_at(lane, q)) =
+              *reinterpret_cast<uint4*>(so + swz<RB16>(lane, q)) =
                   make_uint4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
           }
           if (zout) {
 #pragma unroll
             for (int q = 0; q < EPI_COLS / 4; q++)
-              *reinterpret_cast<float4*>(sz + sw128_at(lane, q)) =
+              *reinterpret_cast<float4*>(sz + swz<RB32>(lane, q)) =
                   make_float4(zz[4 * q], zz[4 * q + 1], zz[4 * q + 2], zz[4 * q + 3]);
           }
           fence_async_shared();
@@ -502,23 +530,23 @@ __global__ void __launch_bounds__(THREADS, 1)
         released = true;
       };
       uint32_t va[EPI_COLS], vb[EPI_COLS];
-      tmem_load32(tbase + (uint32_t)cbeg, va);
-      tmem_wait32(va);
+      tmem_load(tbase + (uint32_t)cbeg, va);
+      tmem_wait(va);
 #pragma unroll 1
       for (int c = cbeg; c < cend && ok; c += 2 * EPI_COLS) {
         const bool more = c + EPI_COLS < cend, more2 = c + 2 * EPI_COLS < cend;
         if (more)
-          tmem_load32(tbase + (uint32_t)(c + EPI_COLS), vb);
+          tmem_load(tbase + (uint32_t)(c + EPI_COLS), vb);
         else
           release();
         ok = step(va, c);
         if (!more) break;
-        tmem_wait32(vb);
+        tmem_wait(vb);
         if (!more2) release();
         if (!ok) break;
-        if (more2) tmem_load32(tbase + (uint32_t)(c + 2 * EPI_COLS), va);
+        if (more2) tmem_load(tbase + (uint32_t)(c + 2 * EPI_COLS), va);
         ok = step(vb, c + EPI_COLS);
-        if (more2) tmem_wait32(va);
+        if (more2) tmem_wait(va);
       }
       if (!released && ok) release();
     }

@@ -54,20 +54,24 @@ bool tensor_map(CUtensorMap* m, const void* p, uint64_t rows, uint64_t cols, uin
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// A tensor map for the epilogue's 32-row x 32-column pieces of an output (or of z) [rows][ld]: BF16 with the 64-byte
-// swizzle or FP32 with the 128-byte swizzle, the layouts the epilogue writes its staging in. False when the pointer or
+// A tensor map for the epilogue's 32-row x cols-column pieces of an output (or of z) [rows][ld], BF16 or FP32, with
+// the swizzle of the piece's row bytes (32, 64 or 128), the layouts the epilogue writes its staging in. False when the pointer or
 // the row pitch is not a multiple of 16 bytes or the encoding fails (the epilogue then stores directly, 16 bytes at a
 // time, which asks for the same alignment: the launcher refuses anything less).
-bool piece_map(CUtensorMap* m, const void* p, uint64_t rows, uint64_t cols, uint64_t ld, bool f32) {
+bool piece_map(CUtensorMap* m, const void* p, uint64_t rows, uint64_t cols, uint64_t ld, bool f32, int piece_cols) {
   const uint64_t es = f32 ? 4 : 2;
   if (((uintptr_t)p & 15) || (ld * es) % 16) return false;
   const cuuint64_t dims[2] = {cols, rows};
   const cuuint64_t strides[1] = {ld * es};
-  const cuuint32_t box[2] = {(cuuint32_t)EPI_COLS, 32};
+  const cuuint32_t box[2] = {(cuuint32_t)piece_cols, 32};
+  const uint64_t row_bytes = (uint64_t)piece_cols * es;
+  const CUtensorMapSwizzle sw = row_bytes == 128  ? CU_TENSOR_MAP_SWIZZLE_128B
+                                : row_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                  : CU_TENSOR_MAP_SWIZZLE_32B;
   const cuuint32_t step[2] = {1, 1};
   return g_encode(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
                   const_cast<void*>(p), dims, strides, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  f32 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  sw, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -76,18 +80,18 @@ int g_sms = 0;
 // the column tile of a product with N columns: the widest of 256, 192, 128, 64 that divides N
 int tile_width(int N) { return N % 256 == 0 ? 256 : N % 192 == 0 ? 192 : N % 128 == 0 ? 128 : 64; }
 
-template <int BN, int STAGES, int EPI>
+template <int BN, int STAGES, int EPI, int EW>
 cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& to, const CUtensorMap& tz,
                         int64_t M, int N, int K, const Epi& ep, int* err, cudaStream_t st) {
   // the opt-in shared memory, set once per instance and device (a bit per device; devices past 63 set it every time)
   static std::atomic<unsigned long long> configured{0};
-  constexpr int smem = gemm_smem_bytes<BN, STAGES>();
+  constexpr int smem = gemm_smem_bytes<BN, STAGES, EW>();
   static_assert(smem <= 232448, "more shared memory than a CTA of sm_100a may opt into");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return cudaErrorInvalidDevice;
   const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
   if (!bit || !(configured.load() & bit)) {
-    const cudaError_t e = cudaFuncSetAttribute((const void*)gemm_kernel<BN, STAGES, EPI>,
+    const cudaError_t e = cudaFuncSetAttribute((const void*)gemm_kernel<BN, STAGES, EPI, EW>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     configured.fetch_or(bit);
@@ -99,20 +103,24 @@ cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, const CUte
   }
   const long long tiles = ((M + BM - 1) / BM) * (long long)(N / BN) * ep.splits;
   const int grid = (int)std::min<long long>(tiles, std::max(g_sms, 1));  // persistent: one CTA per SM
-  gemm_kernel<BN, STAGES, EPI><<<grid, THREADS, smem, st>>>(ta, tb, to, tz, (int)M, N, K, ep, err);
+  gemm_kernel<BN, STAGES, EPI, EW><<<grid, EpiShape<EW>::THREADS, smem, st>>>(ta, tb, to, tz, (int)M, N, K, ep, err);
   return cudaGetLastError();
 }
+
+// the epilogue warps of a column tile width and an epilogue
+constexpr int epi_warps(int bn, int epi) { return (void)bn, (void)epi, 8; }
 
 // the kernel for a column tile width and an epilogue
 template <int BN, int STAGES>
 cudaError_t launch_epi(int epi, const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& to,
                        const CUtensorMap& tz, int64_t M, int N, int K, const Epi& ep, int* err, cudaStream_t st) {
   switch (epi) {
-    case V_STORE: return launch_tile<BN, STAGES, V_STORE>(ta, tb, to, tz, M, N, K, ep, err, st);
-    case V_BIAS: return launch_tile<BN, STAGES, V_BIAS>(ta, tb, to, tz, M, N, K, ep, err, st);
-    case V_SILU: return launch_tile<BN, STAGES, V_SILU>(ta, tb, to, tz, M, N, K, ep, err, st);
-    case V_SILU_Z: return launch_tile<BN, STAGES, V_SILU_Z>(ta, tb, to, tz, M, N, K, ep, err, st);
-    default: return launch_tile<BN, STAGES, V_DSILU>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_STORE: return launch_tile<BN, STAGES, V_STORE, epi_warps(BN, V_STORE)>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_BIAS: return launch_tile<BN, STAGES, V_BIAS, epi_warps(BN, V_BIAS)>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_SILU: return launch_tile<BN, STAGES, V_SILU, epi_warps(BN, V_SILU)>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_SILU_Z:
+      return launch_tile<BN, STAGES, V_SILU_Z, epi_warps(BN, V_SILU_Z)>(ta, tb, to, tz, M, N, K, ep, err, st);
+    default: return launch_tile<BN, STAGES, V_DSILU, epi_warps(BN, V_DSILU)>(ta, tb, to, tz, M, N, K, ep, err, st);
   }
 }
 
@@ -148,9 +156,10 @@ int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, in
   memset(&to, 0, sizeof(to));
   memset(&tz, 0, sizeof(tz));
   const uint64_t out_rows = splits > 1 ? (uint64_t)splits * (uint64_t)ep.split_rows : (uint64_t)M;
-  e2.tma = piece_map(&to, ep.out, out_rows, (uint64_t)N, (uint64_t)ep.ldo, f32_out) &&
-           (!uses_z || piece_map(&tz, ep.z, (uint64_t)M, (uint64_t)N, (uint64_t)ep.ldz, true));
   const int epi = variant_of(ep.mode, ep.mode == BIAS_SILU && ep.z != nullptr);
+  const int pcols = epi_warps(bn, epi) == 8 ? EpiShape<8>::COLS : EpiShape<16>::COLS;
+  e2.tma = piece_map(&to, ep.out, out_rows, (uint64_t)N, (uint64_t)ep.ldo, f32_out, pcols) &&
+           (!uses_z || piece_map(&tz, ep.z, (uint64_t)M, (uint64_t)N, (uint64_t)ep.ldz, true, pcols));
   const cudaError_t e = bn == 256   ? launch_epi<256, 3>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
                         : bn == 192 ? launch_epi<192, 4>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
                         : bn == 128 ? launch_epi<128, 5>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
