@@ -3,9 +3,9 @@
 // C[M, N] = A[M, K] B[N, K]^T, A and B row-major BF16 (both K-major), FP32 accumulation in tensor memory, in tiles of
 // 128 x BN: TMA streams the K blocks of A and B into shared-memory stages (128-byte swizzle, tensor maps over this
 // GPU's memory only), one thread issues the tcgen05.mma's (M 128, N BN, K 16 each, four per 64-wide K block) into a
-// TMEM accumulator and hands each stage back with tcgen05.commit, and 8 or 16 warps read the accumulator (tcgen05.ld
-// 32x32b) through the epilogue, which stages each 32-row piece of its outputs in shared memory (32-, 64- or 128-byte
-// swizzle, conflict-free for the row-per-lane writes) and writes it with a TMA store. Every wait on an mbarrier
+// TMEM accumulator and hands each stage back with tcgen05.commit, and eight warps read the accumulator (tcgen05.ld
+// 32x32b) through the epilogue, which stages each 32-row x 32-column piece of its outputs in shared memory (64- or
+// 128-byte swizzle, conflict-free for the row-per-lane writes) and writes it with a TMA store. Every wait on an mbarrier
 // gives up after about a second of clock ticks: the CTA then sets *err, lets its issued copies finish (bounded waits),
 // frees its tensor memory and returns.
 //
@@ -21,23 +21,21 @@
 namespace mxg {
 
 constexpr int BM = 128, BK = 64;
-// The epilogue's shape for EW epilogue warps: 8, two per TMEM lane quarter in 32-column steps, or 16, four per quarter
-// in 16-column steps (half the registers, so that four epilogue warps share each SM sub-partition). Per warp, the
-// staging holds the output piece at 0 (32 rows x COLS FP32, or BF16) and the z piece at 2 KB (FP32); the FP32 outputs
-// (STORE, BIAS) have no z, so the two never overlap in use.
-template <int EW>
-struct EpiShape {
-  static_assert(EW == 8 || EW == 16, "8 or 16 epilogue warps");
-  static constexpr int THREADS = 64 + 32 * EW;  // producer warp, MMA warp, epilogue warps
-  static constexpr int COLS = EW == 8 ? 32 : 16;
-  static constexpr int STAGING = EW == 8 ? 6144 : 4096;
-};
+constexpr int EPI_WARPS = 8;                  // two per TMEM lane quarter, each over half the tile's columns
+constexpr int THREADS = 64 + 32 * EPI_WARPS;  // producer warp, MMA warp, epilogue warps
+constexpr int EPI_COLS = 32;                  // accumulator columns per epilogue step
 enum Epilogue { STORE = 0, BIAS = 1, BIAS_SILU = 2, DSILU = 3 };
 // The kernel is compiled per epilogue (its registers then hold only what that epilogue needs): BIAS_SILU splits into
 // SILU (activation only, the inference pass) and SILU_Z (the pre-activation kept in FP32 too, the training pass).
 enum Variant { V_STORE = 0, V_BIAS = 1, V_SILU = 2, V_SILU_Z = 3, V_DSILU = 4 };
 __host__ __device__ constexpr int variant_of(int mode, bool keep_z) {
   return mode == STORE ? V_STORE : mode == BIAS ? V_BIAS : mode == BIAS_SILU ? (keep_z ? V_SILU_Z : V_SILU) : V_DSILU;
+}
+
+// Staging bytes per epilogue warp: the output piece at 0 (32 rows x 32 columns: 2 KB in BF16, 4 KB in FP32) and, for
+// the epilogues with z, the z piece (FP32, 4 KB) at 2 KB. Less staging leaves room for a deeper ring of A and B stages.
+__host__ __device__ constexpr int staging_bytes(int epi) {
+  return epi == V_SILU ? 2048 : (epi == V_STORE || epi == V_BIAS) ? 4096 : 6144;
 }
 
 struct Epi {
@@ -160,23 +158,8 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 __device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
-// 32 (or 16) consecutive accumulator columns of the warp's 32 TMEM lanes (one row per thread), issued; tmem_wait waits
-// for every load of the thread and ties v's registers to the wait, so that no use of them moves above it.
-__device__ __forceinline__ void tmem_load(uint32_t taddr, uint32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
-      "[%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_wait(uint32_t (&v)[16]) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;"
-               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
-                 "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15])
-               :
-               : "memory");
-}
+// 32 consecutive accumulator columns of the warp's 32 TMEM lanes (one row per thread), issued; tmem_wait waits for
+// every load of the thread and ties v's registers to the wait, so that no use of them moves above it.
 __device__ __forceinline__ void tmem_load(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
@@ -245,9 +228,16 @@ __host__ __device__ constexpr uint32_t tmem_columns(int bn) {
 
 // Shared-memory bytes of one CTA: the stages (1024-aligned), the epilogue warps' staging, the barriers and the TMEM
 // address slot, plus the slack that aligns the dynamic base to 1024 bytes.
-template <int BN, int STAGES, int EW>
-__host__ __device__ constexpr int gemm_smem_bytes() {
-  return STAGES * (BM + BN) * BK * 2 + EW * EpiShape<EW>::STAGING + 8 * (2 * STAGES + 4 + EW) + 16 + 1024;
+__host__ __device__ constexpr int gemm_smem_bytes(int bn, int stages, int epi) {
+  return stages * (BM + bn) * BK * 2 + EPI_WARPS * staging_bytes(epi) + 8 * (2 * stages + 4 + EPI_WARPS) + 16 + 1024;
+}
+
+// The deepest ring of stages (at most 8) that fits one CTA's 227 KB of shared memory beside the epilogue's staging:
+// the bytes in flight between TMA and the tensor core are what hide the loads' latency.
+__host__ __device__ constexpr int stages_for(int bn, int epi) {
+  int s = 8;
+  while (s > 2 && gemm_smem_bytes(bn, s, epi) > 232448) s--;
+  return s;
 }
 
 // Byte offset of 16-byte chunk c of row r in a staging piece of RB-byte rows (32, 64 or 128) as the TMA unit lays out
@@ -260,7 +250,7 @@ __device__ __forceinline__ uint32_t swz(int r, int c) {
 
 // The epilogue's arithmetic on COLS accumulator columns (a, columns col ..) of one row; zz holds z for DSILU.
 // BIAS_SILU leaves z = C + bias in zz and the activation in a.
-template <int EPI, int SFU_EVERY, int EPI_COLS>
+template <int EPI, int SFU_EVERY>
 __device__ __forceinline__ void epilogue_math(const Epi& ep, float (&a)[EPI_COLS], float (&zz)[EPI_COLS], int col) {
   if constexpr (EPI == V_BIAS || EPI == V_SILU || EPI == V_SILU_Z) {
     const float4* b4 = reinterpret_cast<const float4*>(ep.bias + col);
@@ -288,7 +278,6 @@ __device__ __forceinline__ void epilogue_math(const Epi& ep, float (&a)[EPI_COLS
   }
 }
 
-template <int EPI_COLS>
 __device__ __forceinline__ void pack_bf16(const float (&a)[EPI_COLS], uint32_t (&p)[EPI_COLS / 2]) {
 #pragma unroll
   for (int j = 0; j < EPI_COLS / 2; j++) {
@@ -297,18 +286,18 @@ __device__ __forceinline__ void pack_bf16(const float (&a)[EPI_COLS], uint32_t (
   }
 }
 
-// Persistent and warp-specialised: one CTA of 2 + EW warps per SM walks the output tiles (row tiles outer, column
-// tiles inner, so neighbouring tiles share A's rows in L2). Warp 0 (one thread) streams the K blocks of A and B into a
-// ring of STAGES shared-memory stages; warp 1 (one thread) issues the MMAs into one of two TMEM accumulators of BN
-// columns each and commits; warps 2 .. EW + 1 drain the other accumulator through the epilogue (warp w the TMEM lanes
-// 32 (w % 4) .. 32 (w % 4) + 31; the EW / 4 warps of a lane quarter take consecutive slices of the columns) and hand
-// it back, so a tile's epilogue overlaps the next tile's MMAs. With ep.tma, each epilogue warp stages its 32-row
-// output pieces in its own shared memory and stores them with TMA (one bulk group per warp, waited for before the
-// staging is rewritten); DSILU's z pieces come in the same way by TMA loads, one ahead. EPI is the epilogue
-// (Variant); EW the epilogue warps (EpiShape); SFU_EVERY the sigmoid's split between the special-function unit and
-// the FMA pipe.
-template <int BN, int STAGES, int EPI, int EW, int SFU_EVERY = 2>
-__global__ void __launch_bounds__(EpiShape<EW>::THREADS, 1)
+// Persistent and warp-specialised: one CTA of 10 warps per SM walks the output tiles (row tiles outer, column tiles
+// inner, so neighbouring tiles share A's rows in L2). Warp 0 (one thread) streams the K blocks of A and B into a ring
+// of STAGES shared-memory stages; warp 1 (one thread) issues the MMAs into one of two TMEM accumulators of BN columns
+// each and commits; warps 2-9 drain the other accumulator through the epilogue (warp w the TMEM lanes 32 (w % 4) ..
+// 32 (w % 4) + 31, warps 2-5 the left half of the columns and 6-9 the right half) and hand it back, so a tile's
+// epilogue overlaps the next tile's MMAs. With ep.tma, each epilogue warp stages its 32 x 32 output pieces in its own
+// shared memory and stores them with TMA (one bulk group per warp, waited for before the staging is rewritten);
+// DSILU's z pieces come in the same way by TMA loads, one ahead. EPI is the epilogue (Variant); SFU_EVERY the
+// sigmoid's split between the special-function unit and the FMA pipe. (Sixteen epilogue warps in 16-column steps,
+// four per SM sub-partition at 96 registers, were measured no faster.)
+template <int BN, int STAGES, int EPI, int SFU_EVERY = 2>
+__global__ void __launch_bounds__(THREADS, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
                 const __grid_constant__ CUtensorMap to, const __grid_constant__ CUtensorMap tz, int M, int N, int K,
                 Epi ep, int* err) {
@@ -316,10 +305,10 @@ __global__ void __launch_bounds__(EpiShape<EW>::THREADS, 1)
   uint8_t* base = (uint8_t*)(((uintptr_t)gemm_smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* sa = base;                                       // STAGES x [128][64] BF16
   uint8_t* sb = base + STAGES * BM * BK * 2;                // STAGES x [BN][64] BF16
-  constexpr int EPI_COLS = EpiShape<EW>::COLS, STAGING = EpiShape<EW>::STAGING;
-  uint8_t* stg = sb + STAGES * BN * BK * 2;          // EW x STAGING
-  uint64_t* bars = (uint64_t*)(stg + EW * STAGING);  // full[S], empty[S], acc_full[2], acc_empty[2], z[EW]
-  uint32_t* tslot = (uint32_t*)(bars + 2 * STAGES + 4 + EW);
+  constexpr int STAGING = staging_bytes(EPI);
+  uint8_t* stg = sb + STAGES * BN * BK * 2;                 // EPI_WARPS x STAGING
+  uint64_t* bars = (uint64_t*)(stg + EPI_WARPS * STAGING);  // full[S], empty[S], acc_full[2], acc_empty[2], z[8]
+  uint32_t* tslot = (uint32_t*)(bars + 2 * STAGES + 4 + EPI_WARPS);
   const int tid = (int)threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nk = K / BK, tiles_n = N / BN, tiles_mn = ((M + BM - 1) / BM) * tiles_n;
   const int nks = (nk + ep.splits - 1) / ep.splits, tiles = tiles_mn * ep.splits;
@@ -333,9 +322,9 @@ __global__ void __launch_bounds__(EpiShape<EW>::THREADS, 1)
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(accf0 + 8 * b, 1);
-      mbar_init(acce0 + 8 * b, EW);  // one arrival per epilogue warp
+      mbar_init(acce0 + 8 * b, EPI_WARPS);  // one arrival per epilogue warp
     }
-    for (int w = 0; w < EW; w++) mbar_init(zbar0 + 8 * w, 1);
+    for (int w = 0; w < EPI_WARPS; w++) mbar_init(zbar0 + 8 * w, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -401,7 +390,7 @@ __global__ void __launch_bounds__(EpiShape<EW>::THREADS, 1)
     }
   } else if (warp >= 2) {  // epilogue
     const int ew = warp - 2, quarter = warp & 3;
-    constexpr int WCOLS = BN * 4 / EW;  // columns of the warp's slice
+    constexpr int WCOLS = BN / 2;  // columns of the warp's half
     static_assert(WCOLS % EPI_COLS == 0, "the slice is whole steps");
     constexpr int RB16 = EPI_COLS * 2, RB32 = EPI_COLS * 4;  // staging row bytes: BF16 and FP32 pieces
     const int cbeg = (ew >> 2) * WCOLS, cend = cbeg + WCOLS;
@@ -457,7 +446,7 @@ __global__ void __launch_bounds__(EpiShape<EW>::THREADS, 1)
             }
           }
         }
-        epilogue_math<EPI, SFU_EVERY, EPI_COLS>(ep, a, zz, n0 + c);
+        epilogue_math<EPI, SFU_EVERY>(ep, a, zz, n0 + c);
         if (zin && tma) {  // the z piece is consumed: fetch the next one into the same staging
           __syncwarp();
           if (c + EPI_COLS < cend) {

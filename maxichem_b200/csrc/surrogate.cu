@@ -80,18 +80,18 @@ int g_sms = 0;
 // the column tile of a product with N columns: the widest of 256, 192, 128, 64 that divides N
 int tile_width(int N) { return N % 256 == 0 ? 256 : N % 192 == 0 ? 192 : N % 128 == 0 ? 128 : 64; }
 
-template <int BN, int STAGES, int EPI, int EW>
+template <int BN, int EPI>
 cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& to, const CUtensorMap& tz,
                         int64_t M, int N, int K, const Epi& ep, int* err, cudaStream_t st) {
   // the opt-in shared memory, set once per instance and device (a bit per device; devices past 63 set it every time)
   static std::atomic<unsigned long long> configured{0};
-  constexpr int smem = gemm_smem_bytes<BN, STAGES, EW>();
+  constexpr int STAGES = stages_for(BN, EPI), smem = gemm_smem_bytes(BN, STAGES, EPI);
   static_assert(smem <= 232448, "more shared memory than a CTA of sm_100a may opt into");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return cudaErrorInvalidDevice;
   const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
   if (!bit || !(configured.load() & bit)) {
-    const cudaError_t e = cudaFuncSetAttribute((const void*)gemm_kernel<BN, STAGES, EPI, EW>,
+    const cudaError_t e = cudaFuncSetAttribute((const void*)gemm_kernel<BN, STAGES, EPI>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     configured.fetch_or(bit);
@@ -103,24 +103,20 @@ cudaError_t launch_tile(const CUtensorMap& ta, const CUtensorMap& tb, const CUte
   }
   const long long tiles = ((M + BM - 1) / BM) * (long long)(N / BN) * ep.splits;
   const int grid = (int)std::min<long long>(tiles, std::max(g_sms, 1));  // persistent: one CTA per SM
-  gemm_kernel<BN, STAGES, EPI, EW><<<grid, EpiShape<EW>::THREADS, smem, st>>>(ta, tb, to, tz, (int)M, N, K, ep, err);
+  gemm_kernel<BN, STAGES, EPI><<<grid, THREADS, smem, st>>>(ta, tb, to, tz, (int)M, N, K, ep, err);
   return cudaGetLastError();
 }
 
-// the epilogue warps of a column tile width and an epilogue
-constexpr int epi_warps(int bn, int epi) { return (void)bn, (void)epi, 8; }
-
 // the kernel for a column tile width and an epilogue
-template <int BN, int STAGES>
+template <int BN>
 cudaError_t launch_epi(int epi, const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& to,
                        const CUtensorMap& tz, int64_t M, int N, int K, const Epi& ep, int* err, cudaStream_t st) {
   switch (epi) {
-    case V_STORE: return launch_tile<BN, STAGES, V_STORE, epi_warps(BN, V_STORE)>(ta, tb, to, tz, M, N, K, ep, err, st);
-    case V_BIAS: return launch_tile<BN, STAGES, V_BIAS, epi_warps(BN, V_BIAS)>(ta, tb, to, tz, M, N, K, ep, err, st);
-    case V_SILU: return launch_tile<BN, STAGES, V_SILU, epi_warps(BN, V_SILU)>(ta, tb, to, tz, M, N, K, ep, err, st);
-    case V_SILU_Z:
-      return launch_tile<BN, STAGES, V_SILU_Z, epi_warps(BN, V_SILU_Z)>(ta, tb, to, tz, M, N, K, ep, err, st);
-    default: return launch_tile<BN, STAGES, V_DSILU, epi_warps(BN, V_DSILU)>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_STORE: return launch_tile<BN, V_STORE>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_BIAS: return launch_tile<BN, V_BIAS>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_SILU: return launch_tile<BN, V_SILU>(ta, tb, to, tz, M, N, K, ep, err, st);
+    case V_SILU_Z: return launch_tile<BN, V_SILU_Z>(ta, tb, to, tz, M, N, K, ep, err, st);
+    default: return launch_tile<BN, V_DSILU>(ta, tb, to, tz, M, N, K, ep, err, st);
   }
 }
 
@@ -157,13 +153,13 @@ int mx_gemm_launch(const void* A, int lda, const void* B, int ldb, int64_t M, in
   memset(&tz, 0, sizeof(tz));
   const uint64_t out_rows = splits > 1 ? (uint64_t)splits * (uint64_t)ep.split_rows : (uint64_t)M;
   const int epi = variant_of(ep.mode, ep.mode == BIAS_SILU && ep.z != nullptr);
-  const int pcols = epi_warps(bn, epi) == 8 ? EpiShape<8>::COLS : EpiShape<16>::COLS;
+  const int pcols = EPI_COLS;
   e2.tma = piece_map(&to, ep.out, out_rows, (uint64_t)N, (uint64_t)ep.ldo, f32_out, pcols) &&
            (!uses_z || piece_map(&tz, ep.z, (uint64_t)M, (uint64_t)N, (uint64_t)ep.ldz, true, pcols));
-  const cudaError_t e = bn == 256   ? launch_epi<256, 3>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
-                        : bn == 192 ? launch_epi<192, 4>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
-                        : bn == 128 ? launch_epi<128, 5>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
-                                    : launch_epi<64, 7>(epi, ta, tb, to, tz, M, N, K, e2, err, st);
+  const cudaError_t e = bn == 256   ? launch_epi<256>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
+                        : bn == 192 ? launch_epi<192>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
+                        : bn == 128 ? launch_epi<128>(epi, ta, tb, to, tz, M, N, K, e2, err, st)
+                                    : launch_epi<64>(epi, ta, tb, to, tz, M, N, K, e2, err, st);
   return e == cudaSuccess ? MX_OK : MX_ERR_CUDA;
 }
 
