@@ -389,6 +389,7 @@ def run_call(args) -> None:
                    "cells_per_gpu": B, "species": tab.ns, "reactions": tab.nr, "photolysis": tab.nj,
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
                    "accepted_steps_mean": steps_mean, "tries_per_cell": (fresh + retry) / (args.steps + args.warmup) / B,
+                   "us_per_cell_call": ms * 1e3 / B,  # per GPU: the unit of the reference's timings (its README.md:201)
                    "counts": dict(zip(["queue", *abi_counts()], counts)), "spinup": spin, "layout": solver.info,
                    "phase_shares": phases},
         "roofline": {"bound": "fp64", "kernel": "call_kernel (the plain arm)", "achieved": achieved,
