@@ -154,3 +154,32 @@ def test_the_gate_decides_on_the_proposals_measures(small, gpu):
     assert torch.equal(r.x[acc], xp[acc])
     assert gated.counts()["accepted"] == int(want.sum())
     sur.close()
+
+
+def test_what_the_network_gains_over_the_method_without_it(small, gpu):
+    """Train on pairs from the plain solver, calibrate the gate on held-out pairs, then run the gated call on cells of
+    a third seed beside the plain call: the whole call's per-species error stays within rtol 1e-3 at the 99.9th
+    percentile with every cell done (the bar), cells the gate rejects carry Rodas3's result bit for bit, and the gain
+    is the share of cells the network answers (each one a Rodas3 solve saved). On these small synthetic sets the
+    gain is measured, not required: the network's errors of a few percent leave the gate little to accept."""
+    net, solver, data = small
+    sur = sg.Surrogate(solver.ns, solver.nj, solver.tab.atoms, gpu, seed=13)
+    sur.fit(data, epochs=6, batch=1024)
+    held = sg.pairs(solver, 2048, 2, seed=41)
+    cal = sg.calibrate(sur, held, target=1e-3)
+    assert 0.0 <= cal["accept"] <= 1.0 and cal["spread_max"] >= 0.0
+    test = sg.pairs(solver, 2048, 2, seed=43)
+    args = (test.x, test.T, test.P, test.dt, test.h)
+    plain = solver.launch(*args, J=test.J)
+    gated = sg.GatedSolver(solver, sur, spread_max=cal["spread_max"], proj_max=cal["proj_max"], audit_every=64, seed=5)
+    r = gated(*args, J=test.J)
+    big = plain.x > 1e-20
+    rel = ((r.x - plain.x).abs() / plain.x)[big]
+    assert float(torch.quantile(rel.float(), 0.999)) <= 1e-3 and bool(r.done.all())
+    acc = (r.steps == 0) & r.done
+    assert torch.equal(r.x[~acc], plain.x[~acc])
+    gain = float(acc.double().mean())
+    print(f"the network answers {gain:.2%} of the test cells (calibrated on held-out: {cal['accept']:.2%}, "
+          f"spread_max {cal['spread_max']:.2e} dex)")
+    assert gated.counts()["accepted"] == int(acc.sum())
+    sur.close()
