@@ -167,7 +167,7 @@ int mx_call_static(mx_solver* s, const double* x, const double* T, const double*
 #define MX_MIXED_TOL 1.0
 
 /*
- * The arithmetic of later mx_call calls of this solver (north-star form 1; no counterpart in the reference, whose
+ * The arithmetic of later mx_call calls of this solver (mixed precision; no counterpart in the reference, whose
  * solve is FP64 throughout). MX_PRECISION_FP64 (the default): the plain path. MX_PRECISION_MIXED: each try's matrix
  * M0 = I / (gamma h) - Jn is row-scaled by powers of two, factored in FP32 and every stage solve is refined `sweeps`
  * times (1..MX_MIXED_MAX_SWEEPS) against an FP64 residual formed from the rate tables (no FP64 matrix is stored);
@@ -306,7 +306,7 @@ int mx_mole_to_mass(const double* x, const double* mw, const double* mass, int64
                     int32_t* bad, void* stream);
 
 /*
- * The learned part of the call (north-star form 4; no counterpart in the reference). A BF16 MLP surrogate of the
+ * The learned part of the call (no counterpart in the reference). A BF16 MLP surrogate of the
  * per-call solve: features of a cell (log10 x per species floored at 1e-30, log10 T, P, dt and the carried h,
  * log10(J + 1e-30) per branch, standardised, zero-padded to a multiple of 64: kin) -> `layers` hidden layers of width `hidden` (SiLU) ->
  * `heads` output blocks of nt = ns + 1 values (log10 x_out - log10 x_in per species, log10 h_out; standardised),

@@ -1,4 +1,4 @@
-// The learned part of the call (north-star form 4): a BF16 MLP surrogate of the per-call solve, its training on the
+// The learned part of the call: a BF16 MLP surrogate of the per-call solve, its training on the
 // GPU, and the gated call that solves only the cells it cannot vouch for. No counterpart in the reference.
 //
 // Network: the features of a cell (log10 x per species floored at 1e-30, log10 T, P, dt and the carried h,

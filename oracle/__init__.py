@@ -1,8 +1,8 @@
 """TEST INFRASTRUCTURE ONLY: the CPU oracle of the per-call chemistry solve (oracle/mx_oracle.c) and of its tangent
 (oracle/mx_oracle_ad.c) through ctypes.
 
-Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this package: as the checker of the CUDA
-path, or as the timed CPU baseline. The product (maxichem_b200) never imports it.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this package: as the oracle the CUDA path
+is compared with, or as the timed CPU baseline. The product (maxichem_b200) never imports it.
 """
 
 from __future__ import annotations

@@ -1,6 +1,6 @@
 /*
  * TEST INFRASTRUCTURE ONLY: the CPU oracle of the per-call chemistry solve. Only tests/, __graft_entry__.smoke() and
- * bench.py's CPU-baseline leg may load it, and only as the checker or the timed CPU baseline; the product never does.
+ * bench.py's CPU-baseline leg may load it, and only as the oracle or the timed CPU baseline; the product never does.
  *
  * A scalar, one-cell-at-a-time restatement of the reference solver's arithmetic (imalsky/maxichem):
  *   rates            maxichem/kernels/common.cuh:136-242 (law, collision_limit, gibbs_rt, rate_pair, cell_rates)

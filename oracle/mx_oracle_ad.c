@@ -1,7 +1,7 @@
 /*
  * TEST INFRASTRUCTURE ONLY: the CPU oracle of the call's tangent (the forward-mode derivative of one call, the
  * reference's ADSolver.jvp, maxichem/kincuda_ad.py:325-453, contracts in docs/method.md:185-236). Only tests/ load it,
- * as the checker of the CUDA tangent; the product never does.
+ * as the oracle of the CUDA tangent; the product never does.
  *
  * Dual numbers (value, tangent) carried through the oracle's own call (mx_oracle.c): every operation of its primal
  * arithmetic, in its order, on the value parts, so the values are the primal oracle's bits, and each operation's

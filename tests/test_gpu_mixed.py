@@ -1,6 +1,6 @@
 """The mixed-precision call (FP32 row-scaled factors, FP64 residual refinement) against the FP64 path on the GPU.
 
-The bar (the north star's): per-species relative error against FP64 within rtol 1e-3 at the 99.9th percentile over
+The bar: per-species relative error against FP64 within rtol 1e-3 at the 99.9th percentile over
 species above 1e-20, zero guard failures (no cell left failed: drifted cells are recomputed in FP64 by the recovery),
 element shares kept to 1e-11, on samples of the 69-species column grid
 (settled 300 s calls and cold starts) and of the 91-species sulfur network (600 s calls). Also: a try's refined stages
