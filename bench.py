@@ -64,7 +64,7 @@ def parse() -> argparse.Namespace:
                    help="time the call with its tangent (jvp, --directions of them) or its adjoint (vjp) instead")
     p.add_argument("--directions", type=int, default=1, help="tangent directions of --derivative jvp")
     p.add_argument("--frozen", action="store_true", help="--derivative with adapt=False (the accepted steps held)")
-    p.add_argument("--arms", default="fp64,learned",
+    p.add_argument("--arms", default="fp64,learned,mixed",
                    help="comma list of fp64, learned (the surrogate's gated call), mixed (FP32 factors)")
     p.add_argument("--train-cells", type=int, default=1 << 20, help="cells of the surrogate's training pairs")
     p.add_argument("--train-calls", type=int, default=10,
@@ -357,8 +357,16 @@ def run_call(args) -> None:
     if mixed is not None:
         report["mixed"]["escalated_per_call"] = int(mixed.escalated.item()) / (report["mixed"]["steps"] + 3)
         report["mixed"]["counts"] = mixed.fallback
+    # the library's launches in each arm's timed region: the FP64 call (call, recovery, counts); the learned call
+    # (features, the network's layers per 65,536-row chunk, gate, audit, the list-mode call, recovery, counts); the
+    # mixed call (mixed kernel, its hand-back list call, recovery, counts, escalation count)
+    per_call = {"fp64": 3, "mixed": 5}
+    if gated is not None:
+        per_call["learned"] = 6 + (gated.sur.layers + 1) * -(-B // 65536)
+    launches = {arm: per_call[arm] * report[arm].get("steps", args.steps) for arm in report}
     for arm in report:
         report[arm]["cells_per_s"] = replicas.throughput(B, world, report[arm]["ms_per_step"] * 1e-3)
+        report[arm]["gpu_launches"] = launches[arm]
     bar = lambda r: ("accuracy_vs_fp64" not in r or  # noqa: E731
                      (r["accuracy_vs_fp64"]["p999"] <= 1e-3 and r["accuracy_vs_fp64"]["done_all"]))
     headline = max((a for a in report if bar(report[a])), key=lambda a: report[a]["cells_per_s"])
@@ -400,7 +408,7 @@ def run_call(args) -> None:
                      "hbm_frac_of_measured": io_bytes / (report["fp64"]["ms_per_step"] * 1e-3) / 1e9 / HBM_GBS,
                      "peak_source": "measured in-process: FP64 fma chains on every SM (mx_probe_fp64)",
                      "flops_per_step": flop_step},
-        "gpu_launches": 3 * args.steps + (86 * args.steps if "learned" in report else 0),
+        "gpu_launches": sum(launches.values()),
         "clocks": clocks.summary(),
     }  # fmt: skip
     if gated is not None:
