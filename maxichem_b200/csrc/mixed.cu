@@ -176,11 +176,19 @@ __device__ __forceinline__ void residual(const Net& net, const Cell& c, const Ex
   group_sync(bar, gnt);
 }
 
+// F (and u0) at Y by the group gtid of gnt threads (named barrier bar): the plain path's rhs, kept out of line here
+// so that the kernel's three evaluations share one copy of its code (the mixed kernel's code is larger than the plain
+// kernel's, and instruction fetch, not arithmetic, stalled it).
+__device__ __noinline__ double rhs_out_of_line(const Net& net, const Cell& c, const double* Y, bool u0, double nd,
+                                               int gtid, int gnt, int bar) {
+  return rhs(net, c, Y, u0, nd, gtid, gnt, bar);
+}
+
 // The refinement of one stage vector x (right side b): `sweeps` times the FP64 residual (all threads) and its FP32
 // correction with the Sherman-Morrison term (warp 0). Returns on warp 0 the last correction's largest size on the
 // error-control scale rtol |N| + atol.
 template <int R>
-__device__ __forceinline__ double refine(const Net& net, const Cell& c, const Extra& e, double* x, const double* b,
+__device__ __noinline__ double refine(const Net& net, const Cell& c, const Extra& e, double* x, const double* b,
                                          double igh, double c0, double rtol, double atol, int sweeps, int tid, int nt) {
   const int lane = tid & 31, warp = tid >> 5;
   double worst = 0.0;
@@ -270,7 +278,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W)
       const double ha = fmin(s.h, dt - s.t), igh = 1.0 / (GAMMA * ha), ih = 1.0 / ha;
       tries++;
       retries += s.prej ? 1 : 0;
-      const double ntot = rhs(net, c, c.N, true, nd, tid, nt);  // F, u0 in U, n at N
+      const double ntot = rhs_out_of_line(net, c, c.N, true, nd, tid, nt, 0);  // F, u0 in U, n at N
       for (int i = tid; i <= ns; i += nt) e.nN[i] = c.n[i];
       jacobian_mixed(net, c, e, tid, nt);
       // w = u0 - Jn N / ntot (jacobian_times_x, call.cuh:61-79), in FP64 from the rate tables
@@ -315,7 +323,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W)
         solve32<R>(net, e, c.K2, lane);
         sherman(net, c.K2, c.U, c0, lane);
       } else {
-        rhs(net, c, c.Y, false, nd, tid - 32, nt - 32, 1);
+        rhs_out_of_line(net, c, c.Y, false, nd, tid - 32, nt - 32, 1);
       }
       __syncthreads();
       worst = fmax(worst, refine<R>(net, c, e, c.K2, e.B, igh, c0, a.rtol, a.atol, sweeps, tid, nt));
@@ -334,7 +342,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W)
       worst = fmax(worst, refine<R>(net, c, e, c.K3, e.B, igh, c0, a.rtol, a.atol, sweeps, tid, nt));
       for (int i = tid; i < ns; i += nt) c.Y[i] = c.N[i] + 2.0 * c.K1[i] + c.K3[i];
       __syncthreads();
-      rhs(net, c, c.Y, false, nd, tid, nt);
+      rhs_out_of_line(net, c, c.Y, false, nd, tid, nt, 0);
       mark(PH_STAGE3);
       if (warp == 0) {  // stage 4
         for (int i = lane; i < ns; i += 32) {
