@@ -25,6 +25,9 @@
 
 using namespace mx;
 
+// Shared memory the mixed kernel's cells may take on one SM (bytes); the rest of the unified 256 KB stays L1.
+constexpr int MIXED_SMEM_BUDGET = 164 * 1024;
+
 namespace {
 
 enum { PH_RATES, PH_RHS_JAC, PH_LU, PH_STAGE12, PH_STAGE3, PH_STAGE4, PH_CONTROL, PH_OUTPUT, PH_COUNT };
@@ -176,12 +179,16 @@ __device__ __forceinline__ void residual(const Net& net, const Cell& c, const Ex
   group_sync(bar, gnt);
 }
 
-// F (and u0) at Y by the group gtid of gnt threads (named barrier bar): the plain path's rhs, kept out of line here
-// so that the kernel's three evaluations share one copy of its code (the mixed kernel's code is larger than the plain
-// kernel's, and instruction fetch, not arithmetic, stalled it).
-__device__ __noinline__ double rhs_out_of_line(const Net& net, const Cell& c, const double* Y, bool u0, double nd,
-                                               int gtid, int gnt, int bar) {
-  return rhs(net, c, Y, u0, nd, gtid, gnt, bar);
+// F (and u0) at Y: the plain path's rhs, kept out of line here so that the kernel's three evaluations share one copy
+// of its code (the mixed kernel's code is larger than the plain kernel's, and instruction fetch, not arithmetic,
+// stalled it). Two forms with fixed barriers (a barrier id known only at run time would make the kernel reserve all
+// sixteen named barriers and cost it a CTA per SM): the whole CTA (barrier 0), and warps 1 .. W - 1 (barrier 1).
+__device__ __noinline__ double rhs_cta(const Net& net, const Cell& c, const double* Y, bool u0, double nd, int tid,
+                                       int nt) {
+  return rhs(net, c, Y, u0, nd, tid, nt, 0);
+}
+__device__ __noinline__ void rhs_tail(const Net& net, const Cell& c, const double* Y, double nd, int gtid, int gnt) {
+  rhs(net, c, Y, false, nd, gtid, gnt, 1);
 }
 
 // The refinement of one stage vector x (right side b): `sweeps` times the FP64 residual (all threads) and its FP32
@@ -278,7 +285,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W)
       const double ha = fmin(s.h, dt - s.t), igh = 1.0 / (GAMMA * ha), ih = 1.0 / ha;
       tries++;
       retries += s.prej ? 1 : 0;
-      const double ntot = rhs_out_of_line(net, c, c.N, true, nd, tid, nt, 0);  // F, u0 in U, n at N
+      const double ntot = rhs_cta(net, c, c.N, true, nd, tid, nt);  // F, u0 in U, n at N
       for (int i = tid; i <= ns; i += nt) e.nN[i] = c.n[i];
       jacobian_mixed(net, c, e, tid, nt);
       // w = u0 - Jn N / ntot (jacobian_times_x, call.cuh:61-79), in FP64 from the rate tables
@@ -323,7 +330,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W)
         solve32<R>(net, e, c.K2, lane);
         sherman(net, c.K2, c.U, c0, lane);
       } else {
-        rhs_out_of_line(net, c, c.Y, false, nd, tid - 32, nt - 32, 1);
+        rhs_tail(net, c, c.Y, nd, tid - 32, nt - 32);
       }
       __syncthreads();
       worst = fmax(worst, refine<R>(net, c, e, c.K2, e.B, igh, c0, a.rtol, a.atol, sweeps, tid, nt));
@@ -342,7 +349,7 @@ __global__ void __launch_bounds__(32 * W, 20 / W)
       worst = fmax(worst, refine<R>(net, c, e, c.K3, e.B, igh, c0, a.rtol, a.atol, sweeps, tid, nt));
       for (int i = tid; i < ns; i += nt) c.Y[i] = c.N[i] + 2.0 * c.K1[i] + c.K3[i];
       __syncthreads();
-      rhs_out_of_line(net, c, c.Y, false, nd, tid, nt, 0);
+      rhs_cta(net, c, c.Y, false, nd, tid, nt);
       mark(PH_STAGE3);
       if (warp == 0) {  // stage 4
         for (int i = lane; i < ns; i += 32) {
@@ -637,9 +644,25 @@ int mx_mixed_prepare(mx_solver* s, int n_pieces, char* err, size_t errlen) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)s->mixed_list, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)s->mixed_smem);
+  // Shared memory for at most the cells that fit 164 KB, the rest of the SM's 256 KB left to L1 for the rate tables and
+  // term streams every try reads (measured at 69 species: 4 cells a SM with 92 KB of L1 ran the call 6 % faster than
+  // 5 cells with 28 KB); the carveout is a percentage of the SM's shared-memory maximum.
+  int per_sm_max = 0, reserved = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, s->device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, s->device);
+  int cells = 1;
+  if (e == cudaSuccess) {
+    const size_t per_cell = s->mixed_smem + (size_t)reserved;
+    cells = std::max(1, (int)((size_t)MIXED_SMEM_BUDGET / per_cell));
+    const int percent = std::min(100, (int)((100 * (size_t)cells * per_cell + per_sm_max - 1) / per_sm_max));
+    for (const void* f : {(const void*)s->mixed, (const void*)s->mixed_prof, (const void*)s->mixed_debug,
+                          (const void*)s->mixed_list})
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
+  }
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->mixed_ctas, (const void*)s->mixed, 32 * s->warps,
                                                       s->mixed_smem);
+  if (e == cudaSuccess) s->mixed_ctas = std::min(s->mixed_ctas, cells);
   if (e == cudaSuccess && s->mixed_ctas < 1) e = cudaErrorInvalidConfiguration;
   if (e != cudaSuccess) {
     set_error(err, errlen, "mx_create: the mixed-precision kernel: %s", cudaGetErrorString(e));
